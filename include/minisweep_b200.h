@@ -1,0 +1,343 @@
+/*
+ * minisweep_b200.h -- C ABI of the B200-native KBA sweep library
+ * (libminisweep_b200.so).
+ *
+ * The library is a drop-in for the sweep path of olcf/minisweep: it exports the
+ * reference's Env / Arguments / Dimensions / Pointer / Quantities / Sweeper C
+ * API with the same names, argument meaning and error behaviour (Insist ->
+ * message on stderr + exit(EXIT_FAILURE)), so the reference's own driver
+ * sources (src/4_driver/runner.c, sweep.c, tester.c) compile against these
+ * headers unchanged and link against this library instead of libsweeper.
+ * The mirror headers in this directory (env.h, sweeper.h, ...) all include
+ * this file, so the reference's #include lines resolve here.
+ *
+ * Every sweep runs on one B200 (sm_100a): there is no CPU path.  Functions
+ * whose name ends in _status return an error code instead of exiting; they
+ * and the *_device entry points have no counterpart in the reference.
+ *
+ * Compile-time sizes follow the reference: NM (moments) defaults to 16 and is
+ * set with -DNM_VALUE=...; NU (unknowns) is fixed at 4 by this library.
+ * The library itself handles NM in {4, 8, 16} at run time (Dimensions.nm).
+ *
+ * Reference interfaces are cited as file:line within olcf/minisweep.
+ */
+#ifndef MINISWEEP_B200_H
+#define MINISWEEP_B200_H
+
+#include <stddef.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*====================================================================== types
+ * src/1_base/types_kernels.h:17-53 */
+typedef double P;
+typedef int Bool_t;
+enum { Bool_true = (1 == 1), Bool_false = (0 == 1) };
+static inline P P_zero(void) { return (P)0; }
+static inline P P_one(void) { return (P)1; }
+
+#ifndef TARGET_HD
+#define TARGET_HD
+#endif
+#ifndef TARGET_G
+#define TARGET_G
+#endif
+
+/* src/1_base/env_assert.h:19-40: Insist always checks (message + exit),
+ * Assert is assert() unless NDEBUG. */
+void insist_(const char* condition_string, const char* file, int line);
+#define Insist(condition) \
+  (void)((condition) || (insist_(#condition, __FILE__, __LINE__), 0))
+#ifndef NDEBUG
+#include <assert.h>
+#define Assert(v) assert(v)
+#else
+#define Assert(v)
+#endif
+#define Static_Assert(condition) { int a[(condition) ? 1 : -1]; (void)a; }
+
+/*=============================================================== definitions
+ * src/2_sweeper_base/definitions_kernels.h:21-64 */
+enum { NDIM = 3 };
+enum { DIM_X = 0 };
+enum { DIM_Y = 1 };
+enum { DIM_Z = 2 };
+enum { NOCTANT = 8 };
+enum { DIR_UP = +1 };
+enum { DIR_DN = -1 };
+enum { DIR_HI = +1 };
+enum { DIR_LO = -1 };
+static inline int Dir_x(int octant) { return octant & (1 << 0) ? (int)DIR_DN : (int)DIR_UP; }
+static inline int Dir_y(int octant) { return octant & (1 << 1) ? (int)DIR_DN : (int)DIR_UP; }
+static inline int Dir_z(int octant) { return octant & (1 << 2) ? (int)DIR_DN : (int)DIR_UP; }
+static inline int Dir_inc(int dir) { return dir; }
+static inline int imin(const int i, const int j) { return i < j ? i : j; }
+static inline int imax(const int i, const int j) { return i > j ? i : j; }
+
+/*================================================================ dimensions
+ * src/2_sweeper_base/dimensions_kernels.h:24-56 */
+#ifdef NU_VALUE
+#if NU_VALUE != 4
+#error "libminisweep_b200 is built for NU = 4 unknowns per cell/moment/group"
+#endif
+#endif
+enum { NU = 4 };
+#ifdef NM_VALUE
+enum { NM = NM_VALUE };
+#else
+enum { NM = 16 };
+#endif
+
+typedef struct {
+  int ncell_x;
+  int ncell_y;
+  int ncell_z;
+  int ne;
+  int nm;
+  int na;
+} Dimensions;
+
+/* src/2_sweeper_base/dimensions.h:28-57 */
+Dimensions Dimensions_null(void);
+size_t Dimensions_size_state(const Dimensions dims, int nu);
+size_t Dimensions_size_state_angles(const Dimensions dims, int nu);
+size_t Dimensions_size_facexy(const Dimensions dims, int nu, int noctant_per_block);
+size_t Dimensions_size_facexz(const Dimensions dims, int nu, int noctant_per_block);
+size_t Dimensions_size_faceyz(const Dimensions dims, int nu, int noctant_per_block);
+
+/*================================================================= arguments
+ * src/1_base/arguments.h:33-88 -- read-once integer flags */
+typedef struct {
+  int argc;
+  char** argv_unconsumed;
+  char* argstring;
+} Arguments;
+
+Arguments Arguments_null(void);
+void Arguments_create(Arguments* args, int argc, char** argv);
+void Arguments_create_from_string(Arguments* args, const char* argstring);
+void Arguments_destroy(Arguments* args);
+Bool_t Arguments_exists(const Arguments* args, const char* arg_name);
+int Arguments_consume_int_(Arguments* args, const char* arg_name);
+int Arguments_consume_int_or_default(Arguments* args, const char* arg_name,
+                                     int default_value);
+Bool_t Arguments_are_all_consumed(const Arguments* args);
+
+/*======================================================================= env
+ * src/1_base/env_types.h:54-70, env.h:46-80, env_mpi.h, env_cuda.h.
+ * One process drives one GPU: the process grid is 1 x 1. */
+typedef int Comm_t;
+typedef int Request_t;
+typedef void* Stream_t; /* a cudaStream_t */
+typedef double Timer;
+
+typedef struct {
+  int nproc_x_;
+  int nproc_y_;
+  int tag_;
+  Bool_t is_proc_active_;
+  Bool_t is_using_device_;
+  Stream_t stream_kernel_faces_;
+  int device_;
+  int pad;
+} Env;
+
+Env Env_null(void);
+void Env_initialize(Env* env, int argc, char** argv);
+void Env_set_values(Env* env, Arguments* args);
+void Env_finalize(Env* env);
+Bool_t Env_is_proc_master(Env* env);
+Timer Env_get_time(Env* env);
+Timer Env_get_synced_time(Env* env);
+int Env_nproc_x(const Env* env);
+int Env_nproc_y(const Env* env);
+int Env_nproc(const Env* env);
+Bool_t Env_is_proc_active(const Env* env);
+int Env_tag(const Env* env);
+void Env_increment_tag(Env* env, int value);
+int Env_proc(const Env* env, int proc_x, int proc_y);
+int Env_proc_x(const Env* env, int proc);
+int Env_proc_y(const Env* env, int proc);
+int Env_proc_this(const Env* env);
+int Env_proc_x_this(const Env* env);
+int Env_proc_y_this(const Env* env);
+void Env_mpi_barrier(Env* env);
+double Env_sum_d(Env* env, double value);
+P Env_sum_P(Env* env, P value);
+Bool_t Env_cuda_is_using_device(const Env* const env);
+Bool_t Env_cuda_last_call_succeeded(void);
+Stream_t Env_cuda_stream_kernel_faces(Env* env);
+void Env_cuda_stream_wait(Env* env, Stream_t stream);
+
+/* src/1_base/env_cuda.h host/device memory helpers */
+int* malloc_host_int(size_t n);
+P* malloc_host_P(size_t n);
+P* malloc_host_pinned_P(size_t n);
+P* malloc_device_P(size_t n);
+void free_host_int(int* p);
+void free_host_P(P* p);
+void free_host_pinned_P(P* p);
+void free_device_P(P* p);
+void cuda_copy_host_to_device_P(P* p_d, P* p_h, size_t n);
+void cuda_copy_device_to_host_P(P* p_h, P* p_d, size_t n);
+
+/*=================================================================== pointer
+ * src/1_base/pointer_kernels.h:33-41, pointer.h:28-112: a host array with an
+ * optional device mirror. */
+enum { IS_USING_DEVICE = Bool_true, IS_NOT_USING_DEVICE = Bool_false };
+enum { IS_PINNED = Bool_true, IS_NOT_PINNED = Bool_false };
+
+typedef struct {
+  size_t n_;
+  P* h_;
+  P* d_;
+  Bool_t is_using_device_;
+  Bool_t is_pinned_;
+  Bool_t is_alias_;
+} Pointer;
+
+static inline P* Pointer_h(Pointer* p) { return p->h_; }
+static inline const P* Pointer_const_h(const Pointer* p) { return p->h_; }
+static inline P* Pointer_d(Pointer* p) { return p->d_; }
+static inline const P* Pointer_const_d(const Pointer* p) { return p->d_; }
+static inline P* Pointer_active(Pointer* p) { return p->is_using_device_ ? p->d_ : p->h_; }
+static inline P* Pointer_const_active(const Pointer* p) { return p->is_using_device_ ? p->d_ : p->h_; }
+
+Pointer Pointer_null(void);
+void Pointer_create(Pointer* p, size_t n, Bool_t is_using_device);
+void Pointer_create_alias(Pointer* p, Pointer* source, size_t base, size_t n);
+void Pointer_set_pinned(Pointer* p, Bool_t is_pinned);
+void Pointer_destroy(Pointer* p);
+void Pointer_allocate_h_(Pointer* p);
+void Pointer_allocate_d_(Pointer* p);
+void Pointer_allocate(Pointer* p);
+void Pointer_deallocate_h_(Pointer* p);
+void Pointer_deallocate_d_(Pointer* p);
+void Pointer_deallocate(Pointer* p);
+void Pointer_update_h(Pointer* p);
+void Pointer_update_d(Pointer* p);
+void Pointer_update_h_stream(Pointer* p, Stream_t stream);
+void Pointer_update_d_stream(Pointer* p, Stream_t stream);
+
+/*================================================================ quantities
+ * src/3_sweeper/quantities_testing_kernels.h:35-46 (struct),
+ * quantities_testing.h:27-90 (API): the built-in deterministic problem. */
+typedef struct {
+  Pointer a_from_m; /* [octant][im][ia], im stride NM  */
+  Pointer m_from_a; /* [octant][ia][im]                */
+  int* ix_base_vals;
+  int* iy_base_vals;
+  int ix_base;
+  int iy_base;
+  int ncell_x_g;
+  int ncell_y_g;
+  int ncell_z_g;
+} Quantities;
+
+void Quantities_create(Quantities* quan, const Dimensions dims, Env* env);
+void Quantities_destroy(Quantities* quan);
+void Quantities_init_am_matrices_(Quantities* quan, const Dimensions dims, Env* env);
+void Quantities_init_decomp_(Quantities* quan, const Dimensions dims, Env* env);
+double Quantities_flops_per_solve(const Dimensions dims);
+P Quantities_init_state(const Quantities* quan, int ix, int iy, int iz, int ie,
+                        int im, int iu, const Dimensions dims);
+
+/*========================================================== array operations
+ * src/2_sweeper_base/array_operations.h:27-55 (host arrays, FP64). */
+void initialize_state(P* const v, const Dimensions dims, const int nu,
+                      const Quantities* const quan);
+void initialize_state_zero(P* const v, const Dimensions dims, const int nu);
+void get_state_norms(const P* const vi, const P* const vo, const Dimensions dims,
+                     const int nu, P* const normsqp, P* const normsqdiffp,
+                     Env* const env);
+void copy_vector(P* const vo, const P* const vi, const size_t n);
+
+/*=================================================================== sweeper
+ * src/3_sweeper/sweeper_kba.h:34-257.  The struct keeps the reference's
+ * flag-derived fields (all accepted and validated as the reference does,
+ * sweeper_kba_c.h:44-287); the device state lives behind impl_. */
+typedef struct {
+  Dimensions dims;
+  Dimensions dims_b;
+  Dimensions dims_g;
+  int nblock_z;
+  int nblock_octant;
+  int noctant_per_block;
+  int nsemiblock;
+  int ncell_x_per_subblock;
+  int ncell_y_per_subblock;
+  int ncell_z_per_subblock;
+  int nthread_e;
+  int nthread_octant;
+  int nthread_x;
+  int nthread_y;
+  int nthread_z;
+  Bool_t is_face_comm_async;
+  int precision;    /* 0: FP64 plain; 1: mixed precision (--precision 1) */
+  void* impl_;
+} Sweeper;
+
+/* sweeper_kba.h:66-70 */
+Sweeper Sweeper_null(void);
+/* sweeper_kba.h:74-80 / sweeper_kba_c.h:44-287: consumes the sweeper flags */
+void Sweeper_create(Sweeper* sweeper, Dimensions dims, const Quantities* quan,
+                    Env* env, Arguments* args);
+/* sweeper_kba.h:84-87 / sweeper_kba_c.h:292-329 */
+void Sweeper_destroy(Sweeper* sweeper, Env* env);
+/* sweeper_kba.h:243-249 / sweeper_kba_c.h:588-845: vo = sweep(vi).  Reads vi
+ * from its host copy and leaves vo's host copy complete on return, as the
+ * reference does (its step loop copies every z-block back). */
+void Sweeper_sweep(Sweeper* sweeper, Pointer* vo, Pointer* vi,
+                   const Quantities* quan, Env* env);
+/* sweeper_kba.h:253-257 */
+int Sweeper_noctant_per_block(const Sweeper* sweeper);
+
+/*------------------------------------------------ extensions (no reference
+ * counterpart).  Status codes: 0 ok, <0 error; the message is available from
+ * msb_last_error().  These never exit the process. */
+enum {
+  MSB_OK = 0,
+  MSB_ERR_ARG = -1,        /* invalid flag / size                          */
+  MSB_ERR_CUDA = -2,       /* CUDA runtime error                           */
+  MSB_ERR_TIMEOUT = -3,    /* a bounded device spin-wait gave up           */
+  MSB_ERR_UNSUPPORTED = -4 /* size outside the compiled kernel variants    */
+};
+const char* msb_last_error(void);
+int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Quantities* quan,
+                          Env* env, Arguments* args);
+int Sweeper_sweep_status(Sweeper* sweeper, Pointer* vo, Pointer* vi,
+                         const Quantities* quan, Env* env);
+/* vo_d/vi_d: device arrays in the reference state layout.  Asynchronous on the
+ * Env's stream; the status of the device work is checked by
+ * Sweeper_sync_status. */
+int Sweeper_sweep_device(Sweeper* sweeper, double* vo_d, const double* vi_d,
+                         const Quantities* quan, Env* env);
+int Sweeper_sync_status(Sweeper* sweeper, Env* env);
+/* Device-side FP64 checksums of two device state arrays (same sums as
+ * get_state_norms). */
+int msb_state_norms_device(const double* vi_d, const double* vo_d, size_t n,
+                           double* normsq, double* normsqdiff, Env* env);
+/* Device-side built-in initial state (same values as initialize_state). */
+int msb_initialize_state_device(double* v_d, Dimensions dims, Env* env);
+/* Kernel statistics of the last sweep: number of tasks, kernel launches. */
+int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int* nlaunch);
+/* Copy of the schedule (one record of MSB_TASK_INTS ints per task, in launch
+ * order) for host-side checks; returns the task count, or <0. */
+enum { MSB_TASK_INTS = 16 };
+long long Sweeper_debug_tasks(const Sweeper* sweeper, int* out, long long max_tasks);
+/* Test hook: time budget (ns) of every device wait in the next sweeps;
+ * 0 = default (4 s). */
+int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit);
+/* The schedule the sweeper would build for these sizes and tile shape,
+ * without touching a GPU (host-side checks). */
+long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int* out, long long max_tasks);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MINISWEEP_B200_H */

@@ -1,0 +1,239 @@
+"""minisweep_b200 -- B200-native KBA sweep behind the minisweep C API.
+
+The product is ``libminisweep_b200.so`` (C ABI declared in
+``include/minisweep_b200.h``).  This module is a thin ctypes binding used by
+the tests and the benchmark: it mirrors the reference's C structs and calls
+the library's entry points.  There is no Python or CPU compute path; if the
+library is missing, importing the binding raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libminisweep_b200.so")
+NU = 4
+NOCTANT = 8
+TASK_INTS = 16
+
+MSB_OK, MSB_ERR_ARG, MSB_ERR_CUDA, MSB_ERR_TIMEOUT, MSB_ERR_UNSUPPORTED = 0, -1, -2, -3, -4
+
+
+def build() -> None:
+    """Compile the CUDA library in-tree for sm_100a."""
+    subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "csrc"), "-j8"])
+
+
+class Dimensions(ctypes.Structure):
+    _fields_ = [("ncell_x", ctypes.c_int), ("ncell_y", ctypes.c_int), ("ncell_z", ctypes.c_int),
+                ("ne", ctypes.c_int), ("nm", ctypes.c_int), ("na", ctypes.c_int)]
+
+
+class Arguments(ctypes.Structure):
+    _fields_ = [("argc", ctypes.c_int), ("argv_unconsumed", ctypes.POINTER(ctypes.c_char_p)),
+                ("argstring", ctypes.c_char_p)]
+
+
+class Env(ctypes.Structure):
+    _fields_ = [("nproc_x_", ctypes.c_int), ("nproc_y_", ctypes.c_int), ("tag_", ctypes.c_int),
+                ("is_proc_active_", ctypes.c_int), ("is_using_device_", ctypes.c_int),
+                ("stream_kernel_faces_", ctypes.c_void_p), ("device_", ctypes.c_int), ("pad", ctypes.c_int)]
+
+
+class Pointer(ctypes.Structure):
+    _fields_ = [("n_", ctypes.c_size_t), ("h_", ctypes.c_void_p), ("d_", ctypes.c_void_p),
+                ("is_using_device_", ctypes.c_int), ("is_pinned_", ctypes.c_int), ("is_alias_", ctypes.c_int)]
+
+
+class Quantities(ctypes.Structure):
+    _fields_ = [("a_from_m", Pointer), ("m_from_a", Pointer), ("ix_base_vals", ctypes.c_void_p),
+                ("iy_base_vals", ctypes.c_void_p), ("ix_base", ctypes.c_int), ("iy_base", ctypes.c_int),
+                ("ncell_x_g", ctypes.c_int), ("ncell_y_g", ctypes.c_int), ("ncell_z_g", ctypes.c_int)]
+
+
+class Sweeper(ctypes.Structure):
+    _fields_ = [("dims", Dimensions), ("dims_b", Dimensions), ("dims_g", Dimensions)] + [
+        (n, ctypes.c_int) for n in (
+            "nblock_z", "nblock_octant", "noctant_per_block", "nsemiblock", "ncell_x_per_subblock",
+            "ncell_y_per_subblock", "ncell_z_per_subblock", "nthread_e", "nthread_octant", "nthread_x",
+            "nthread_y", "nthread_z", "is_face_comm_async", "precision")] + [("impl_", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() (CUDA library not built)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, D = ctypes.POINTER, ctypes.c_double
+        L.msb_last_error.restype = ctypes.c_char_p
+        L.Env_initialize.argtypes = [P(Env), ctypes.c_int, ctypes.c_void_p]
+        L.Env_set_values.argtypes = [P(Env), P(Arguments)]
+        L.Env_finalize.argtypes = [P(Env)]
+        L.Arguments_create_from_string.argtypes = [P(Arguments), ctypes.c_char_p]
+        L.Arguments_destroy.argtypes = [P(Arguments)]
+        L.Arguments_consume_int_or_default.argtypes = [P(Arguments), ctypes.c_char_p, ctypes.c_int]
+        L.Arguments_are_all_consumed.argtypes = [P(Arguments)]
+        L.Quantities_create.argtypes = [P(Quantities), Dimensions, P(Env)]
+        L.Quantities_destroy.argtypes = [P(Quantities)]
+        L.Sweeper_create_status.argtypes = [P(Sweeper), Dimensions, P(Quantities), P(Env), P(Arguments)]
+        L.Sweeper_destroy.argtypes = [P(Sweeper), P(Env)]
+        L.Sweeper_sweep_status.argtypes = [P(Sweeper), P(Pointer), P(Pointer), P(Quantities), P(Env)]
+        L.Sweeper_sweep_device.argtypes = [P(Sweeper), ctypes.c_void_p, ctypes.c_void_p, P(Quantities), P(Env)]
+        L.Sweeper_sync_status.argtypes = [P(Sweeper), P(Env)]
+        L.Sweeper_last_stats.argtypes = [P(Sweeper), P(ctypes.c_longlong), P(ctypes.c_int)]
+        L.Sweeper_debug_tasks.argtypes = [P(Sweeper), P(ctypes.c_int), ctypes.c_longlong]
+        L.Sweeper_debug_tasks.restype = ctypes.c_longlong
+        L.Sweeper_set_spin_limit.argtypes = [P(Sweeper), ctypes.c_longlong]
+        L.msb_state_norms_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, P(D), P(D), P(Env)]
+        L.msb_initialize_state_device.argtypes = [ctypes.c_void_p, Dimensions, P(Env)]
+        L.msb_schedule_tasks.argtypes = [ctypes.c_int] * 6 + [P(ctypes.c_int), ctypes.c_longlong]
+        L.msb_schedule_tasks.restype = ctypes.c_longlong
+        L.initialize_state.argtypes = [P(D), Dimensions, ctypes.c_int, P(Quantities)]
+        L.get_state_norms.argtypes = [P(D), P(D), Dimensions, ctypes.c_int, P(D), P(D), P(Env)]
+        _lib = L
+    return _lib
+
+
+class SweepError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _check(rc: int) -> None:
+    if rc != MSB_OK:
+        raise SweepError(rc, lib().msb_last_error().decode())
+
+
+def last_error() -> str:
+    return lib().msb_last_error().decode()
+
+
+def schedule(nx, ny, nz, ne, tx=4, ty=2) -> np.ndarray:
+    """Task table (ntask x 16 ints) the sweeper builds; no GPU needed."""
+    L = lib()
+    n = L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, None, 0)
+    if n < 0:
+        raise SweepError(int(n), last_error())
+    out = np.zeros((n, TASK_INTS), dtype=np.int32)
+    L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+    return out
+
+
+class Problem:
+    """One sweep problem driven through the reference-compatible C API:
+    Env + Quantities (built-in) + Sweeper created from a reference flag string."""
+
+    def __init__(self, argstring: str, nm: int = 16):
+        L = lib()
+        self.env = Env()
+        L.Env_initialize(ctypes.byref(self.env), 0, None)
+        self.args = Arguments()
+        L.Arguments_create_from_string(ctypes.byref(self.args), argstring.encode())
+        L.Env_set_values(ctypes.byref(self.env), ctypes.byref(self.args))
+        g = lambda name, d: L.Arguments_consume_int_or_default(ctypes.byref(self.args), name.encode(), d)
+        self.dims = Dimensions(g("--ncell_x", 5), g("--ncell_y", 5), g("--ncell_z", 5), g("--ne", 30), nm,
+                               g("--na", 33))
+        self.niterations = g("--niterations", 1)
+        self.quan = Quantities()
+        L.Quantities_create(ctypes.byref(self.quan), self.dims, ctypes.byref(self.env))
+        self.sweeper = Sweeper()
+        rc = L.Sweeper_create_status(ctypes.byref(self.sweeper), self.dims, ctypes.byref(self.quan),
+                                     ctypes.byref(self.env), ctypes.byref(self.args))
+        if rc != MSB_OK:
+            msg = last_error()
+            L.Quantities_destroy(ctypes.byref(self.quan))
+            L.Arguments_destroy(ctypes.byref(self.args))
+            L.Env_finalize(ctypes.byref(self.env))
+            raise SweepError(rc, msg)
+        if not L.Arguments_are_all_consumed(ctypes.byref(self.args)):
+            self.close()
+            raise SweepError(MSB_ERR_ARG, "Invalid argument detected.")
+        self.nstate = (self.dims.ncell_x * self.dims.ncell_y * self.dims.ncell_z * self.dims.ne * nm * NU)
+        self._closed = False
+
+    # ---------------------------------------------------------------- data
+    def matrices(self):
+        """Host copies of a_from_m and m_from_a (reference layouts)."""
+        n = self.dims.nm * self.dims.na * NOCTANT
+        a = np.ctypeslib.as_array(ctypes.cast(self.quan.a_from_m.h_, ctypes.POINTER(ctypes.c_double)), (n,))
+        m = np.ctypeslib.as_array(ctypes.cast(self.quan.m_from_a.h_, ctypes.POINTER(ctypes.c_double)), (n,))
+        return a, m
+
+    def set_matrices(self, a_from_m: np.ndarray, m_from_a: np.ndarray) -> None:
+        a, m = self.matrices()
+        a[:] = a_from_m
+        m[:] = m_from_a
+
+    def init_state(self) -> np.ndarray:
+        v = np.zeros(self.nstate)
+        lib().initialize_state(v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.dims, NU,
+                               ctypes.byref(self.quan))
+        return v
+
+    # ---------------------------------------------------------------- runs
+    def sweep_host(self, vi: np.ndarray) -> np.ndarray:
+        """vo = sweep(vi) through Sweeper_sweep's reference semantics (host in, host out)."""
+        vi = np.ascontiguousarray(vi, dtype=np.float64)
+        vo = np.zeros_like(vi)
+        pvi = Pointer(vi.size, vi.ctypes.data, None, 0, 0, 0)
+        pvo = Pointer(vo.size, vo.ctypes.data, None, 0, 0, 0)
+        _check(lib().Sweeper_sweep_status(ctypes.byref(self.sweeper), ctypes.byref(pvo), ctypes.byref(pvi),
+                                          ctypes.byref(self.quan), ctypes.byref(self.env)))
+        return vo
+
+    def sweep_device(self, vo_ptr: int, vi_ptr: int) -> None:
+        """Enqueue vo = sweep(vi) on device arrays (async on self.stream)."""
+        _check(lib().Sweeper_sweep_device(ctypes.byref(self.sweeper), ctypes.c_void_p(vo_ptr),
+                                          ctypes.c_void_p(vi_ptr), ctypes.byref(self.quan), ctypes.byref(self.env)))
+
+    def sync(self) -> None:
+        _check(lib().Sweeper_sync_status(ctypes.byref(self.sweeper), ctypes.byref(self.env)))
+
+    def norms_device(self, vi_ptr: int, vo_ptr: int):
+        s, d = ctypes.c_double(), ctypes.c_double()
+        _check(lib().msb_state_norms_device(ctypes.c_void_p(vi_ptr), ctypes.c_void_p(vo_ptr), self.nstate,
+                                            ctypes.byref(s), ctypes.byref(d), ctypes.byref(self.env)))
+        return s.value, d.value
+
+    def init_state_device(self, v_ptr: int) -> None:
+        _check(lib().msb_initialize_state_device(ctypes.c_void_p(v_ptr), self.dims, ctypes.byref(self.env)))
+
+    @property
+    def stream(self) -> int:
+        return self.env.stream_kernel_faces_ or 0
+
+    def tasks(self) -> np.ndarray:
+        L = lib()
+        n = L.Sweeper_debug_tasks(ctypes.byref(self.sweeper), None, 0)
+        out = np.zeros((n, TASK_INTS), dtype=np.int32)
+        L.Sweeper_debug_tasks(ctypes.byref(self.sweeper), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+        return out
+
+    def set_timeout_ns(self, ns: int) -> None:
+        _check(lib().Sweeper_set_spin_limit(ctypes.byref(self.sweeper), ns))
+
+    def close(self) -> None:
+        if getattr(self, "_closed", True):
+            return
+        L = lib()
+        L.Sweeper_destroy(ctypes.byref(self.sweeper), ctypes.byref(self.env))
+        L.Quantities_destroy(ctypes.byref(self.quan))
+        L.Arguments_destroy(ctypes.byref(self.args))
+        L.Env_finalize(ctypes.byref(self.env))
+        self._closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

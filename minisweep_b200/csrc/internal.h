@@ -1,0 +1,71 @@
+// internal.h -- declarations shared by the library's translation units.
+#pragma once
+
+#include <cstddef>
+#include <vector>
+
+#include "minisweep_b200.h"
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
+
+namespace msb {
+
+int set_error(int code, const char* fmt, ...);
+#ifdef __CUDACC__
+int cuda_check(cudaError_t e, const char* what);
+#endif
+void insist_status(int rc, const char* what);
+
+int scale_space(int ix, int iy, int iz);
+int scale_energy(int ie);
+int scale_unknown(int iu);
+int scale_angle(int ia);
+void build_am_matrices(int nm, int na, double* a, double* m);
+
+// State layout of the reference (array_accessors_kernels.h:64-89):
+// im fastest, then iu, ix, iy, ie, and iz slowest.
+inline size_t ind_state(const Dimensions& d, int nu, int ix, int iy, int iz, int ie, int im, int iu) {
+  return im + (size_t)d.nm * (iu + (size_t)nu * (ix + (size_t)d.ncell_x *
+              (iy + (size_t)d.ncell_y * (ie + (size_t)d.ne * (size_t)iz))));
+}
+
+// ------------------------------------------------------------------ schedule
+// One task = one octant sweeping one xy tile (TX x TY cells, the full z extent
+// of its region) of one region for one group pair.  Regions are the 2x2x2
+// halves of the grid; in phase p octant o sweeps region (o ^ p), so the eight
+// octants of a phase touch disjoint cells and every region is visited by the
+// octants in phase order (which fixes the order of the vo accumulation).
+enum TaskField {
+  TK_OCT = 0, TK_PHASE, TK_GP, TK_X0, TK_X1, TK_Y0, TK_Y1, TK_Z0, TK_Z1,
+  TK_FLAGS, TK_DEP_X, TK_DEP_Y, TK_DEP_Z, TK_DEP_VO, TK_DEP_MODE, TK_LEVEL
+};
+static_assert(TK_LEVEL + 1 == MSB_TASK_INTS, "task record size");
+
+enum TaskFlags {
+  TF_X_IN = 1 << 0,   // x-upwind face comes from the global face buffer
+  TF_Y_IN = 1 << 1,   //   (otherwise: domain boundary value)
+  TF_Z_IN = 1 << 2,
+  TF_X_OUT = 1 << 3,  // x-downwind face goes to the global face buffer
+  TF_Y_OUT = 1 << 4,  //   (otherwise: domain boundary, nobody reads it)
+  TF_Z_OUT = 1 << 5,
+  TF_FIRST = 1 << 6   // first visitor of its cells in this sweep: vo = ...
+};
+enum DepMode {
+  DM_X_PLANE = 1 << 0,  // DEP_X is a same-phase neighbour: wait plane by plane
+  DM_Y_PLANE = 1 << 1   //   (otherwise wait for completion before starting)
+};
+
+struct Schedule {
+  int nx = 0, ny = 0, nz = 0, ngp = 0, tx = 0, ty = 0;
+  std::vector<int> rec;  // ntask * MSB_TASK_INTS, topological launch order
+  long long ntask() const { return (long long)rec.size() / MSB_TASK_INTS; }
+};
+
+// Builds the task DAG in a topological order: (phase, group pair, level of
+// the tile along the octant's sweep direction, octant, tile).  Returns 0 or
+// an error code.
+int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, Schedule& out);
+
+}  // namespace msb

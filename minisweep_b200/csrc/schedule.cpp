@@ -1,0 +1,196 @@
+// schedule.cpp -- host-side construction of the on-device sweep schedule.
+//
+// Replaces the reference's host step loop (sweeper_kba_c.h:588-845) and its
+// StepScheduler (stepscheduler_kba.c:80-372).  Instead of numbered KBA steps
+// driven from the host, the sweep is a DAG of tasks that one persistent kernel
+// executes in the order built here, each task waiting on per-task progress
+// counters in global memory.
+//
+// Race freedom of the vo accumulation follows the reference's semiblock idea
+// (sweeper_kba_c_kernels.h:1118-1159), applied to the whole grid: the grid is
+// cut into 2x2x2 regions and in phase p octant o works in region o^p.  Bit b
+// of p says whether the region lies on the downwind half along axis b for
+// that octant, so each octant visits its regions in a valid upwind order, and
+// within one phase the eight octants are in eight different regions.  The
+// tiles of one region are visited by the octants in phase order, which is the
+// order in which vo is accumulated (phase 0 writes, later phases add).
+#include <algorithm>
+#include <array>
+#include <cstdint>
+#include <unordered_map>
+
+#include "internal.h"
+
+namespace msb {
+
+namespace {
+
+struct Range {
+  int lo, hi;  // [lo, hi)
+  bool empty() const { return hi <= lo; }
+};
+
+Range half(int n, int bit) {
+  const int h = (n + 1) / 2;
+  return bit ? Range{h, n} : Range{0, h};
+}
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+struct Key {
+  int phase, gp, level, oct, ity, itx;
+  bool operator<(const Key& o) const {
+    if (phase != o.phase) return phase < o.phase;
+    if (gp != o.gp) return gp < o.gp;
+    if (level != o.level) return level < o.level;
+    if (oct != o.oct) return oct < o.oct;
+    if (ity != o.ity) return ity < o.ity;
+    return itx < o.itx;
+  }
+};
+
+inline uint64_t pack(int phase, int oct, int gp, int itx, int ity) {
+  return ((uint64_t)phase << 60) | ((uint64_t)oct << 56) | ((uint64_t)gp << 36) |
+         ((uint64_t)itx << 18) | (uint64_t)ity;
+}
+
+}  // namespace
+
+int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, Schedule& out) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || ngp <= 0 || tx <= 0 || ty <= 0)
+    return set_error(MSB_ERR_ARG, "schedule: invalid sizes");
+  if (ngp >= (1 << 20) || nx >= (1 << 18) || ny >= (1 << 18))
+    return set_error(MSB_ERR_ARG, "schedule: sizes too large");
+  out = Schedule();
+  out.nx = nx;
+  out.ny = ny;
+  out.nz = nz;
+  out.ngp = ngp;
+  out.tx = tx;
+  out.ty = ty;
+
+  struct Item {
+    Key key;
+    std::array<int, MSB_TASK_INTS> r;
+    uint64_t id;
+  };
+  std::vector<Item> items;
+
+  for (int p = 0; p < NOCTANT; ++p)
+    for (int o = 0; o < NOCTANT; ++o) {
+      const int reg = o ^ p;
+      const Range rx = half(nx, reg & 1), ry = half(ny, (reg >> 1) & 1), rz = half(nz, (reg >> 2) & 1);
+      if (rx.empty() || ry.empty() || rz.empty()) continue;
+      const int dx = (o & 1) ? -1 : 1, dy = (o & 2) ? -1 : 1;
+      const int ntx = ceil_div(rx.hi - rx.lo, tx), nty = ceil_div(ry.hi - ry.lo, ty);
+      for (int gp = 0; gp < ngp; ++gp)
+        for (int ity = 0; ity < nty; ++ity)
+          for (int itx = 0; itx < ntx; ++itx) {
+            Item it;
+            it.r.fill(-1);
+            int* r = it.r.data();
+            r[TK_OCT] = o;
+            r[TK_PHASE] = p;
+            r[TK_GP] = gp;
+            r[TK_X0] = rx.lo + itx * tx;
+            r[TK_X1] = std::min(rx.hi, rx.lo + (itx + 1) * tx);
+            r[TK_Y0] = ry.lo + ity * ty;
+            r[TK_Y1] = std::min(ry.hi, ry.lo + (ity + 1) * ty);
+            r[TK_Z0] = rz.lo;
+            r[TK_Z1] = rz.hi;
+            const int ax = dx > 0 ? itx : ntx - 1 - itx;
+            const int ay = dy > 0 ? ity : nty - 1 - ity;
+            r[TK_LEVEL] = ax + ay;
+            it.key = Key{p, gp, ax + ay, o, ity, itx};
+            it.id = pack(p, o, gp, itx, ity);
+            items.push_back(it);
+          }
+    }
+
+  std::sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.key < b.key; });
+  std::unordered_map<uint64_t, int> index;
+  index.reserve(items.size() * 2);
+  for (size_t i = 0; i < items.size(); ++i) index[items[i].id] = (int)i;
+  auto find = [&](int p, int o, int gp, int itx, int ity) -> int {
+    auto f = index.find(pack(p, o, gp, itx, ity));
+    return f == index.end() ? -1 : f->second;
+  };
+
+  out.rec.resize(items.size() * MSB_TASK_INTS);
+  for (size_t i = 0; i < items.size(); ++i) {
+    int* r = items[i].r.data();
+    const int o = r[TK_OCT], p = r[TK_PHASE], gp = r[TK_GP];
+    const int reg = o ^ p;
+    const int dx = (o & 1) ? -1 : 1, dy = (o & 2) ? -1 : 1, dz = (o & 4) ? -1 : 1;
+    const Range rx = half(nx, reg & 1), ry = half(ny, (reg >> 1) & 1);
+    const int ntx = ceil_div(rx.hi - rx.lo, tx), nty = ceil_div(ry.hi - ry.lo, ty);
+    const int itx = (r[TK_X0] - rx.lo) / tx, ity = (r[TK_Y0] - ry.lo) / ty;
+    int flags = 0, mode = 0;
+
+    // ---- x: upwind neighbour tile, inside the region or across its boundary
+    {
+      const bool first_in_reg = dx > 0 ? itx == 0 : itx == ntx - 1;
+      const bool last_in_reg = dx > 0 ? itx == ntx - 1 : itx == 0;
+      if (!first_in_reg) {
+        r[TK_DEP_X] = find(p, o, gp, itx - dx, ity);
+        mode |= DM_X_PLANE;
+      } else {
+        // the other x-half is upwind iff this region is on the downwind half
+        const bool downwind_half = ((p >> 0) & 1) != 0;
+        if (downwind_half) {
+          const int preg = reg ^ 1;
+          const Range px = half(nx, preg & 1);
+          const int pntx = ceil_div(px.hi - px.lo, tx);
+          r[TK_DEP_X] = find(p ^ 1, o, gp, dx > 0 ? pntx - 1 : 0, ity);
+        }
+      }
+      if (r[TK_DEP_X] >= 0) flags |= TF_X_IN;
+      const bool has_down = !last_in_reg || (((p >> 0) & 1) == 0 && !half(nx, (reg ^ 1) & 1).empty());
+      if (has_down) flags |= TF_X_OUT;
+    }
+    // ---- y
+    {
+      const bool first_in_reg = dy > 0 ? ity == 0 : ity == nty - 1;
+      const bool last_in_reg = dy > 0 ? ity == nty - 1 : ity == 0;
+      if (!first_in_reg) {
+        r[TK_DEP_Y] = find(p, o, gp, itx, ity - dy);
+        mode |= DM_Y_PLANE;
+      } else {
+        const bool downwind_half = ((p >> 1) & 1) != 0;
+        if (downwind_half) {
+          const int preg = reg ^ 2;
+          const Range py = half(ny, (preg >> 1) & 1);
+          const int pnty = ceil_div(py.hi - py.lo, ty);
+          r[TK_DEP_Y] = find(p ^ 2, o, gp, itx, dy > 0 ? pnty - 1 : 0);
+        }
+      }
+      if (r[TK_DEP_Y] >= 0) flags |= TF_Y_IN;
+      const bool has_down = !last_in_reg || (((p >> 1) & 1) == 0 && !half(ny, ((reg ^ 2) >> 1) & 1).empty());
+      if (has_down) flags |= TF_Y_OUT;
+    }
+    // ---- z: the task spans its region's z extent; the neighbour is the same
+    // tile in the other z-half
+    {
+      const bool downwind_half = ((p >> 2) & 1) != 0;
+      if (downwind_half) r[TK_DEP_Z] = find(p ^ 4, o, gp, itx, ity);
+      if (r[TK_DEP_Z] >= 0) flags |= TF_Z_IN;
+      if (!downwind_half && !half(nz, ((reg ^ 4) >> 2) & 1).empty()) flags |= TF_Z_OUT;
+      (void)dz;
+    }
+    // ---- vo order: previous visitor of this tile (phase p-1, octant reg^(p-1))
+    if (p == 0) {
+      flags |= TF_FIRST;
+    } else {
+      r[TK_DEP_VO] = find(p - 1, reg ^ (p - 1), gp, itx, ity);
+      if (r[TK_DEP_VO] < 0) return set_error(MSB_ERR_ARG, "schedule: missing vo predecessor");
+    }
+    r[TK_FLAGS] = flags;
+    r[TK_DEP_MODE] = mode;
+    for (int d = TK_DEP_X; d <= TK_DEP_VO; ++d)
+      if (r[d] >= (int)i) return set_error(MSB_ERR_ARG, "schedule: dependency not topological");
+    std::copy(r, r + MSB_TASK_INTS, out.rec.begin() + i * MSB_TASK_INTS);
+  }
+  return MSB_OK;
+}
+
+}  // namespace msb

@@ -1,0 +1,359 @@
+// sweeper.cu -- the Sweeper C API on one B200.
+//
+// Sweeper_create (sweeper_kba_c.h:44-287) consumes and validates the same
+// flags as the reference, then builds the task schedule and the device
+// buffers (face planes per octant, schedule, progress counters).
+// Sweeper_sweep (sweeper_kba_c.h:588-845) is one persistent kernel launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <memory>
+#include <new>
+
+#include "internal.h"
+#include "sweep_fp64.cuh"
+
+namespace msb {
+
+namespace {
+
+using KernelFn = void (*)(const Fp64Params);
+
+struct Variant {
+  KernelFn fn = nullptr;
+  size_t smem = 0;
+  int tx = 0, ty = 0, nch = 0;
+};
+
+template <int NM_, int NCH, int TX, int TY>
+Variant make_variant() {
+  Variant v;
+  v.fn = sweep_fp64_kernel<NM_, NCH, TX, TY>;
+  v.smem = Fp64Cfg<NM_, NCH, TX, TY>::smem_bytes();
+  v.tx = TX;
+  v.ty = TY;
+  v.nch = NCH;
+  return v;
+}
+
+template <int NM_>
+Variant pick_nch(int nch) {
+  switch (nch) {
+    case 1: return make_variant<NM_, 1, 4, 2>();
+    case 2: return make_variant<NM_, 2, 4, 2>();
+    case 3:
+    case 4: return make_variant<NM_, 4, 2, 2>();
+    default: return Variant();
+  }
+}
+
+Variant pick_variant(int nm, int na) {
+  const int nch = (na + 31) / 32;
+  switch (nm) {
+    case 4: return pick_nch<4>(nch);
+    case 8: return pick_nch<8>(nch);
+    case 16: return pick_nch<16>(nch);
+    default: return Variant();
+  }
+}
+
+constexpr long long kDefaultTimeoutNs = 4000000000LL;  // 4 s per wait
+
+}  // namespace
+
+struct SweeperImpl {
+  Dimensions dims{};
+  int ngp = 0;
+  Variant var;
+  Schedule sched;
+  int grid = 0;
+  int* d_tasks = nullptr;
+  int* d_sync = nullptr;
+  size_t sync_ints = 0;
+  double* d_face[3] = {nullptr, nullptr, nullptr};  // xy, xz, yz
+  size_t face_doubles[3] = {0, 0, 0};
+  double* d_afm = nullptr;
+  double* d_mfa = nullptr;
+  double* d_vi = nullptr;  // staging for host-only Pointers
+  double* d_vo = nullptr;
+  long long timeout_ns = kDefaultTimeoutNs;
+  int nlaunch = 0;
+  int* h_status = nullptr;  // pinned copy of the status words
+
+  ~SweeperImpl() {
+    cudaFree(d_tasks);
+    cudaFree(d_sync);
+    for (auto& f : d_face) cudaFree(f);
+    cudaFree(d_afm);
+    cudaFree(d_mfa);
+    cudaFree(d_vi);
+    cudaFree(d_vo);
+    if (h_status) cudaFreeHost(h_status);
+  }
+};
+
+static int impl_create(SweeperImpl& S, const Dimensions& dims) {
+  S.dims = dims;
+  if (dims.ncell_x <= 0 || dims.ncell_y <= 0 || dims.ncell_z <= 0 || dims.ne <= 0 || dims.na <= 0)
+    return set_error(MSB_ERR_ARG, "invalid dimensions");
+  S.var = pick_variant(dims.nm, dims.na);
+  if (!S.var.fn)
+    return set_error(MSB_ERR_UNSUPPORTED, "no kernel variant for nm=%d na=%d (nm in {4,8,16}, na <= 128)",
+                     dims.nm, dims.na);
+  S.ngp = (dims.ne + 1) / 2;
+  int rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, S.var.tx, S.var.ty, S.sched);
+  if (rc) return rc;
+  const long long ntask = S.sched.ntask();
+  if (ntask >= (1LL << 31) - SY_PROGRESS) return set_error(MSB_ERR_ARG, "too many tasks");
+
+  if ((rc = cuda_check(cudaMalloc(&S.d_tasks, S.sched.rec.size() * sizeof(int)), "cudaMalloc tasks"))) return rc;
+  if ((rc = cuda_check(cudaMemcpy(S.d_tasks, S.sched.rec.data(), S.sched.rec.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice), "copy tasks")))
+    return rc;
+  S.sync_ints = SY_PROGRESS + (size_t)ntask;
+  if ((rc = cuda_check(cudaMalloc(&S.d_sync, S.sync_ints * sizeof(int)), "cudaMalloc sync"))) return rc;
+  if ((rc = cuda_check(cudaMallocHost(&S.h_status, 8 * sizeof(int)), "cudaMallocHost status"))) return rc;
+
+  const size_t ent = (size_t)S.var.nch * 256;
+  const size_t per = (size_t)NOCTANT * S.ngp * ent;
+  S.face_doubles[0] = per * dims.ncell_y * dims.ncell_x;
+  S.face_doubles[1] = per * dims.ncell_z * dims.ncell_x;
+  S.face_doubles[2] = per * dims.ncell_z * dims.ncell_y;
+  for (int f = 0; f < 3; ++f)
+    if ((rc = cuda_check(cudaMalloc(&S.d_face[f], S.face_doubles[f] * sizeof(double)), "cudaMalloc faces")))
+      return rc;
+  const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
+  if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
+  if ((rc = cuda_check(cudaMalloc(&S.d_mfa, nmat * sizeof(double)), "cudaMalloc m_from_a"))) return rc;
+
+  if ((rc = cuda_check(cudaFuncSetAttribute(S.var.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S.var.smem),
+                       "cudaFuncSetAttribute")))
+    return rc;
+  int dev = 0, nsm = 0, occ = 0;
+  if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+  if ((rc = cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rc;
+  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, S.var.fn, S.var.tx * S.var.ty * 32,
+                                                                     S.var.smem),
+                       "occupancy")))
+    return rc;
+  if (occ < 1) return set_error(MSB_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
+  S.grid = (int)std::min<long long>(ntask, (long long)nsm * occ);
+  return MSB_OK;
+}
+
+// Launches one sweep: vo_d = sweep(vi_d), asynchronously on `stream`.
+static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
+                      const double* afm_d, const double* mfa_d, cudaStream_t stream) {
+  int rc;
+  const size_t nmat = (size_t)S.dims.nm * S.dims.na * NOCTANT;
+  if (afm_d && mfa_d) {
+    if ((rc = cuda_check(cudaMemcpyAsync(S.d_afm, afm_d, nmat * sizeof(double), cudaMemcpyDeviceToDevice, stream),
+                         "copy a_from_m")))
+      return rc;
+    if ((rc = cuda_check(cudaMemcpyAsync(S.d_mfa, mfa_d, nmat * sizeof(double), cudaMemcpyDeviceToDevice, stream),
+                         "copy m_from_a")))
+      return rc;
+  } else {
+    if ((rc = cuda_check(cudaMemcpyAsync(S.d_afm, afm_h, nmat * sizeof(double), cudaMemcpyHostToDevice, stream),
+                         "copy a_from_m")))
+      return rc;
+    if ((rc = cuda_check(cudaMemcpyAsync(S.d_mfa, mfa_h, nmat * sizeof(double), cudaMemcpyHostToDevice, stream),
+                         "copy m_from_a")))
+      return rc;
+  }
+  if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
+  Fp64Params P;
+  P.vi = vi_d;
+  P.vo = vo_d;
+  P.afm = S.d_afm;
+  P.mfa = S.d_mfa;
+  P.fxy = S.d_face[0];
+  P.fxz = S.d_face[1];
+  P.fyz = S.d_face[2];
+  P.tasks = S.d_tasks;
+  P.ntask = S.sched.ntask();
+  P.nx = S.dims.ncell_x;
+  P.ny = S.dims.ncell_y;
+  P.nz = S.dims.ncell_z;
+  P.ne = S.dims.ne;
+  P.na = S.dims.na;
+  P.ngp = S.ngp;
+  P.sy.sync = S.d_sync;
+  P.sy.timeout_ns = S.timeout_ns;
+  S.var.fn<<<S.grid, S.var.tx * S.var.ty * 32, S.var.smem, stream>>>(P);
+  if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
+                       "status copy")))
+    return rc;
+  S.nlaunch = 1;
+  return MSB_OK;
+}
+
+static int impl_sync(SweeperImpl& S, cudaStream_t stream) {
+  int rc;
+  if ((rc = cuda_check(cudaStreamSynchronize(stream), "sweep"))) return rc;
+  const int err = S.h_status[SY_ERROR];
+  if (err == MSB_ERR_TIMEOUT)
+    return set_error(MSB_ERR_TIMEOUT, "a device wait ran out of time (task %d); sweep aborted", S.h_status[SY_ERRTASK]);
+  if (err) return set_error(err, "device error %d", err);
+  return MSB_OK;
+}
+
+}  // namespace msb
+
+using msb::SweeperImpl;
+
+static SweeperImpl* impl_of(const Sweeper* s) { return static_cast<SweeperImpl*>(s->impl_); }
+static cudaStream_t stream_of(Env* env) { return env ? (cudaStream_t)env->stream_kernel_faces_ : nullptr; }
+
+extern "C" Sweeper Sweeper_null(void) {
+  Sweeper s;
+  memset(&s, 0, sizeof s);
+  return s;
+}
+
+extern "C" int Sweeper_noctant_per_block(const Sweeper* sweeper) { return sweeper->noctant_per_block; }
+
+// Flag handling follows sweeper_kba_c.h:44-233 (names, defaults, checks).
+// Threading flags describe the reference's CPU/GPU thread decomposition; they
+// are validated and recorded but the B200 schedule does not depend on them.
+extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Quantities* quan, Env* env,
+                                     Arguments* args) {
+  *sweeper = Sweeper_null();
+  auto bad = [](const char* m) { return msb::set_error(MSB_ERR_ARG, "%s", m); };
+  sweeper->is_face_comm_async = Arguments_consume_int_or_default(args, "--is_face_comm_async", Bool_true);
+  if (dims.ncell_x <= 0 || dims.ncell_y <= 0 || dims.ncell_z <= 0)
+    return bad("Currently required that all spatial blocks be nonempty");
+  sweeper->nblock_z = Arguments_consume_int_or_default(args, "--nblock_z", 1);
+  if (sweeper->nblock_z <= 0) return bad("Invalid z blocking factor supplied");
+  if (dims.ncell_z % sweeper->nblock_z != 0) return bad("Currently require all blocks have same z dimension");
+  const int dims_b_ncell_z = dims.ncell_z / sweeper->nblock_z;
+  sweeper->nthread_octant = Arguments_consume_int_or_default(args, "--nthread_octant", 1);
+  const int nto = sweeper->nthread_octant;
+  if (!(nto > 0 && nto <= NOCTANT && (nto & (nto - 1)) == 0)) return bad("Invalid thread count supplied");
+  sweeper->noctant_per_block = nto;
+  sweeper->nblock_octant = NOCTANT / nto;
+  const int nsb_default = nto == 8 && sweeper->nblock_z % 2 == 0 ? 4 : nto;
+  sweeper->nsemiblock = Arguments_consume_int_or_default(args, "--nsemiblock", nsb_default);
+  const int nsb = sweeper->nsemiblock;
+  if (!(nsb > 0 && nsb <= NOCTANT && (nsb & (nsb - 1)) == 0)) return bad("Invalid semiblock count supplied");
+  if (!(nsb >= nto || (nto == 8 && sweeper->nblock_z % 2 == 0 && nsb == 4)))
+    return bad("Incomplete set of semiblock steps requires atomic vo update");
+  sweeper->ncell_x_per_subblock = Arguments_consume_int_or_default(
+      args, "--ncell_x_per_subblock", nsb >= 2 ? (dims.ncell_x + 1) / 2 : dims.ncell_x);
+  if (sweeper->ncell_x_per_subblock <= 0) return bad("Invalid subblock size supplied");
+  sweeper->ncell_y_per_subblock = Arguments_consume_int_or_default(
+      args, "--ncell_y_per_subblock", nsb >= 4 ? (dims.ncell_y + 1) / 2 : dims.ncell_y);
+  if (sweeper->ncell_y_per_subblock <= 0) return bad("Invalid subblock size supplied");
+  sweeper->ncell_z_per_subblock = Arguments_consume_int_or_default(
+      args, "--ncell_z_per_subblock", nsb >= 8 ? (dims_b_ncell_z + 1) / 2 : dims_b_ncell_z);
+  if (sweeper->ncell_z_per_subblock <= 0) return bad("Invalid subblock size supplied");
+  sweeper->dims = dims;
+  sweeper->dims_b = dims;
+  sweeper->dims_b.ncell_z = dims_b_ncell_z;
+  sweeper->dims_g = dims;
+  if (quan) {
+    sweeper->dims_g.ncell_x = quan->ncell_x_g;
+    sweeper->dims_g.ncell_y = quan->ncell_y_g;
+  }
+  sweeper->nthread_e = Arguments_consume_int_or_default(args, "--nthread_e", 1);
+  if (sweeper->nthread_e <= 0) return bad("Invalid thread count supplied.");
+  sweeper->nthread_x = 1;
+  sweeper->nthread_y = Arguments_consume_int_or_default(args, "--nthread_y", 1);
+  if (sweeper->nthread_y <= 0) return bad("Invalid thread count supplied.");
+  sweeper->nthread_z = Arguments_consume_int_or_default(args, "--nthread_z", 1);
+  if (sweeper->nthread_z <= 0) return bad("Invalid thread count supplied.");
+  sweeper->precision = Arguments_consume_int_or_default(args, "--precision", 0);
+  if (sweeper->precision != 0) return msb::set_error(MSB_ERR_UNSUPPORTED, "--precision %d is not available", sweeper->precision);
+  (void)env;
+
+  std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
+  if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
+  const int rc = msb::impl_create(*S, dims);
+  if (rc) return rc;
+  sweeper->impl_ = S.release();
+  return MSB_OK;
+}
+
+extern "C" void Sweeper_create(Sweeper* sweeper, Dimensions dims, const Quantities* quan, Env* env, Arguments* args) {
+  msb::insist_status(Sweeper_create_status(sweeper, dims, quan, env, args), "Sweeper_create");
+}
+
+extern "C" void Sweeper_destroy(Sweeper* sweeper, Env* env) {
+  (void)env;
+  delete impl_of(sweeper);
+  sweeper->impl_ = nullptr;
+}
+
+extern "C" int Sweeper_sweep_device(Sweeper* sweeper, double* vo_d, const double* vi_d, const Quantities* quan,
+                                    Env* env) {
+  SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  if (!vo_d || !vi_d || !quan) return msb::set_error(MSB_ERR_ARG, "null argument");
+  const bool mats_on_dev = quan->a_from_m.d_ && quan->m_from_a.d_;
+  return msb::impl_sweep(*S, vo_d, vi_d, quan->a_from_m.h_, quan->m_from_a.h_,
+                         mats_on_dev ? quan->a_from_m.d_ : nullptr, mats_on_dev ? quan->m_from_a.d_ : nullptr,
+                         stream_of(env));
+}
+
+extern "C" int Sweeper_sync_status(Sweeper* sweeper, Env* env) {
+  SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  return msb::impl_sync(*S, stream_of(env));
+}
+
+// Reference semantics: the sweep reads the host copy of vi and leaves the
+// host copy of vo complete (sweeper_kba_c.h:719-781 stages every z-block).
+extern "C" int Sweeper_sweep_status(Sweeper* sweeper, Pointer* vo, Pointer* vi, const Quantities* quan, Env* env) {
+  SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  const size_t n = Dimensions_size_state(S->dims, NU);
+  if (vi->n_ < n || vo->n_ < n || !vi->h_ || !vo->h_) return msb::set_error(MSB_ERR_ARG, "state arrays too small");
+  cudaStream_t st = stream_of(env);
+  int rc;
+  double* vi_d = vi->d_;
+  double* vo_d = vo->d_;
+  if (!vi_d || !vo_d) {
+    if (!S->d_vi && (rc = msb::cuda_check(cudaMalloc(&S->d_vi, n * sizeof(double)), "cudaMalloc vi"))) return rc;
+    if (!S->d_vo && (rc = msb::cuda_check(cudaMalloc(&S->d_vo, n * sizeof(double)), "cudaMalloc vo"))) return rc;
+    if (!vi_d) vi_d = S->d_vi;
+    if (!vo_d) vo_d = S->d_vo;
+  }
+  if ((rc = msb::cuda_check(cudaMemcpyAsync(vi_d, vi->h_, n * sizeof(double), cudaMemcpyHostToDevice, st), "vi H2D")))
+    return rc;
+  if ((rc = Sweeper_sweep_device(sweeper, vo_d, vi_d, quan, env))) return rc;
+  if ((rc = msb::cuda_check(cudaMemcpyAsync(vo->h_, vo_d, n * sizeof(double), cudaMemcpyDeviceToHost, st), "vo D2H")))
+    return rc;
+  return msb::impl_sync(*S, st);
+}
+
+extern "C" void Sweeper_sweep(Sweeper* sweeper, Pointer* vo, Pointer* vi, const Quantities* quan, Env* env) {
+  msb::insist_status(Sweeper_sweep_status(sweeper, vo, vi, quan, env), "Sweeper_sweep");
+}
+
+extern "C" int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int* nlaunch) {
+  const SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  if (ntask) *ntask = S->sched.ntask();
+  if (nlaunch) *nlaunch = S->nlaunch;
+  return MSB_OK;
+}
+
+extern "C" long long Sweeper_debug_tasks(const Sweeper* sweeper, int* out, long long max_tasks) {
+  const SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  const long long n = S->sched.ntask();
+  if (out) {
+    const long long m = std::min(n, max_tasks);
+    memcpy(out, S->sched.rec.data(), (size_t)m * MSB_TASK_INTS * sizeof(int));
+  }
+  return n;
+}
+
+extern "C" int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit) {
+  SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  S->timeout_ns = limit > 0 ? limit : msb::kDefaultTimeoutNs;
+  return MSB_OK;
+}
