@@ -333,9 +333,14 @@ long long Sweeper_debug_tasks(const Sweeper* sweeper, int* out, long long max_ta
 /* Test hook: time budget (ns) of every device wait in the next sweeps;
  * 0 = default (4 s). */
 int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit);
-/* The schedule the sweeper would build for these sizes and tile shape,
- * without touching a GPU (host-side checks). */
-long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int* out, long long max_tasks);
+/* The schedule the sweeper would build for these sizes, tile shape and
+ * group-pair interleave, without touching a GPU (host-side checks). */
+long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int gp_block, int* out,
+                             long long max_tasks);
+/* Measured FP64 throughput of this GPU in TFLOP/s: tensor-core products
+ * (mma.sync f64) and FMA pipe; best of `reps` launches.  The roofline
+ * denominator of the FP64 sweep. */
+int msb_measure_fp64_peak(double* tflops_dmma, double* tflops_dfma, int reps);
 
 #ifdef __cplusplus
 }

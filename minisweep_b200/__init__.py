@@ -95,7 +95,7 @@ def lib() -> ctypes.CDLL:
         L.Sweeper_set_spin_limit.argtypes = [P(Sweeper), ctypes.c_longlong]
         L.msb_state_norms_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, P(D), P(D), P(Env)]
         L.msb_initialize_state_device.argtypes = [ctypes.c_void_p, Dimensions, P(Env)]
-        L.msb_schedule_tasks.argtypes = [ctypes.c_int] * 6 + [P(ctypes.c_int), ctypes.c_longlong]
+        L.msb_schedule_tasks.argtypes = [ctypes.c_int] * 7 + [P(ctypes.c_int), ctypes.c_longlong]
         L.msb_schedule_tasks.restype = ctypes.c_longlong
         L.initialize_state.argtypes = [P(D), Dimensions, ctypes.c_int, P(Quantities)]
         L.get_state_norms.argtypes = [P(D), P(D), Dimensions, ctypes.c_int, P(D), P(D), P(Env)]
@@ -118,14 +118,14 @@ def last_error() -> str:
     return lib().msb_last_error().decode()
 
 
-def schedule(nx, ny, nz, ne, tx=4, ty=2) -> np.ndarray:
+def schedule(nx, ny, nz, ne, tx=4, ty=2, gp_block=1) -> np.ndarray:
     """Task table (ntask x 16 ints) the sweeper builds; no GPU needed."""
     L = lib()
-    n = L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, None, 0)
+    n = L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, gp_block, None, 0)
     if n < 0:
         raise SweepError(int(n), last_error())
     out = np.zeros((n, TASK_INTS), dtype=np.int32)
-    L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+    L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, gp_block, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
     return out
 
 

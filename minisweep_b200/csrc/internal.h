@@ -63,9 +63,15 @@ struct Schedule {
   long long ntask() const { return (long long)rec.size() / MSB_TASK_INTS; }
 };
 
-// Builds the task DAG in a topological order: (phase, group pair, level of
-// the tile along the octant's sweep direction, octant, tile).  Returns 0 or
-// an error code.
-int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, Schedule& out);
+// Builds the task DAG in a topological order: (phase, block of gp_block
+// group pairs, level of the tile along the octant's sweep direction, group
+// pair, octant, tile).  Interleaving gp_block group pairs at each level keeps
+// enough independent tasks in the window of tasks the CTAs hold at once.
+// Returns 0 or an error code.
+int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block, Schedule& out);
+
+// Number of group pairs to interleave so that one level of the schedule holds
+// about `window` tasks.
+int pick_gp_block(int nx, int ny, int ngp, int tx, int ty, int window);
 
 }  // namespace msb

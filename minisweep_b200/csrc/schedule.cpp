@@ -38,11 +38,12 @@ Range half(int n, int bit) {
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 struct Key {
-  int phase, gp, level, oct, ity, itx;
+  int phase, gpb, level, gp, oct, ity, itx;
   bool operator<(const Key& o) const {
     if (phase != o.phase) return phase < o.phase;
-    if (gp != o.gp) return gp < o.gp;
+    if (gpb != o.gpb) return gpb < o.gpb;
     if (level != o.level) return level < o.level;
+    if (gp != o.gp) return gp < o.gp;
     if (oct != o.oct) return oct < o.oct;
     if (ity != o.ity) return ity < o.ity;
     return itx < o.itx;
@@ -56,8 +57,8 @@ inline uint64_t pack(int phase, int oct, int gp, int itx, int ity) {
 
 }  // namespace
 
-int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, Schedule& out) {
-  if (nx <= 0 || ny <= 0 || nz <= 0 || ngp <= 0 || tx <= 0 || ty <= 0)
+int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block, Schedule& out) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || ngp <= 0 || tx <= 0 || ty <= 0 || gp_block <= 0)
     return set_error(MSB_ERR_ARG, "schedule: invalid sizes");
   if (ngp >= (1 << 20) || nx >= (1 << 18) || ny >= (1 << 18))
     return set_error(MSB_ERR_ARG, "schedule: sizes too large");
@@ -101,7 +102,7 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, Schedule& ou
             const int ax = dx > 0 ? itx : ntx - 1 - itx;
             const int ay = dy > 0 ? ity : nty - 1 - ity;
             r[TK_LEVEL] = ax + ay;
-            it.key = Key{p, gp, ax + ay, o, ity, itx};
+            it.key = Key{p, gp / gp_block, ax + ay, gp, o, ity, itx};
             it.id = pack(p, o, gp, itx, ity);
             items.push_back(it);
           }
@@ -191,6 +192,17 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, Schedule& ou
     std::copy(r, r + MSB_TASK_INTS, out.rec.begin() + i * MSB_TASK_INTS);
   }
   return MSB_OK;
+}
+
+int pick_gp_block(int nx, int ny, int ngp, int tx, int ty, int window) {
+  // one region sweep: ntx x nty tiles over ntx + nty - 1 levels, 8 octants
+  const int hx = (nx + 1) / 2, hy = (ny + 1) / 2;
+  const int ntx = ceil_div(hx, tx), nty = ceil_div(hy, ty);
+  const double per_level = 8.0 * ntx * nty / (ntx + nty - 1);
+  int b = (int)((window + per_level - 1) / per_level);
+  if (b < 1) b = 1;
+  if (b > ngp) b = ngp;
+  return b;
 }
 
 }  // namespace msb

@@ -120,9 +120,10 @@ extern "C" int msb_initialize_state_device(double* v_d, Dimensions dims, Env* en
   return msb::cuda_check(cudaGetLastError(), "init state launch");
 }
 
-extern "C" long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int* out, long long max_tasks) {
+extern "C" long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int gp_block, int* out,
+                                        long long max_tasks) {
   msb::Schedule s;
-  const int rc = msb::build_schedule(nx, ny, nz, (ne + 1) / 2, tx, ty, s);
+  const int rc = msb::build_schedule(nx, ny, nz, (ne + 1) / 2, tx, ty, gp_block, s);
   if (rc) return rc;
   const long long n = s.ntask();
   if (out) memcpy(out, s.rec.data(), (size_t)(n < max_tasks ? n : max_tasks) * MSB_TASK_INTS * sizeof(int));

@@ -1,0 +1,637 @@
+// sweep_fp64_ws.cuh -- the plain-FP64 sweep kernel for sm_100a, warp
+// specialised.
+//
+// Replaces the reference's device path: Sweeper_sweep_block_impl_global and
+// everything under it (sweeper_kba_c_kernels.h:30-1383) plus the host step
+// loop that launched it once per KBA step (sweeper_kba_c.h:588-845).
+//
+// Roles inside one CTA (TX*TY compute warps + one producer warpgroup):
+//   loader    grabs tasks (octant, group pair, region tile) from the
+//             topologically ordered table, waits -- with a time budget -- on
+//             the progress counters of the tasks that feed it, and stages the
+//             inputs of every wavefront step into a ring of shared-memory
+//             stages with asynchronous 16-byte copies (vi, the previous vo,
+//             the faces entering the tile).
+//   publisher follows the compute warps' done phases and publishes this
+//             CTA's task progress to global memory, one fence per batch of
+//             finished steps, so no fence sits on the loader's or the compute
+//             warps' path.
+//   compute   warp (a, b) owns cell column (a, b) of the tile and, at step s,
+//             solves plane s - a - b: FP64 tensor-core transforms
+//             (mma.sync m8n8k4 f64), Quantities_solve on registers, the z face
+//             carried in registers, x/y faces passed to the neighbouring warp
+//             through double-buffered shared memory.  They only touch global
+//             memory to write vo and the faces leaving the tile.
+//
+// Stage protocol (global step G counts across tasks):
+//   full[G % NS]  loader: cp.async copies + header; completes when every
+//                 piece has landed; compute waits.
+//   done[G % NS]  each compute warp arrives after its writes of step G and
+//                 waits for the others (the step barrier); the publisher
+//                 consumes the phase, fences, publishes progress, and lets
+//                 the loader reuse the stage.
+//
+// Lane layout (lane l, q = l >> 2, r = l & 3):
+//   column n = q        -> group 2*gp + (q >> 2), unknown q & 3
+//   angles held         -> ia = 32*ch + 8*t + 2*r + i   (t < 4, i < 2)
+//   vi fragment k       -> moment im = (NM/4)*r + k
+//   vo fragment (mt, j) -> moment 8*mt + q, column 2*r + j
+// The accumulator of the first product is the B operand of the second after
+// relabelling the angle index, so psi never leaves registers.
+//
+// Quantities_solve (quantities_testing_kernels.h:337-447) is evaluated in an
+// exactly equivalent 7-operation form: every reassociated factor is a power of
+// two, so each rounded result equals the reference's 12-operation expression.
+#pragma once
+
+#include "sweep_common.cuh"
+
+namespace msb {
+
+struct Fp64Params {
+  const double* vi;
+  double* vo;
+  const double* afm;  // a_from_m [oct][im][ia] (im stride nm)
+  const double* mfa;  // m_from_a [oct][ia][im]
+  double* fxy;        // face planes, one entry = one warp's 8 columns x angles
+  double* fxz;
+  double* fyz;
+  const int* tasks;
+  long long ntask;
+  int nx, ny, nz, ne, na, ngp;
+  SyncArgs sy;
+};
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// ---------------------------------------------------------------- mbarrier
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile(
+      "{\n .reg .b64 st;\n mbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(b))
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile(
+      "{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 st, [%0], %1;\n}" ::"r"(
+          smem_u32(b)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 16-byte asynchronous copy global -> shared (L2 only), and the arrival on an
+// mbarrier once all of this thread's earlier cp.async copies have landed.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait on an mbarrier phase by a whole warp (all lanes poll).  It
+// does not give up when another CTA aborts: inside a CTA every phase that was
+// started is completed (the producer finishes the stages it issued and then
+// posts a stop), so only a time-out ends it early.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const SyncArgs& s, int task) {
+  if (mbar_test(b, parity)) return true;
+  const long long t0 = global_ns();
+  for (;;) {
+    if (mbar_test(b, parity)) return true;
+    if (global_ns() - t0 > s.timeout_ns) {
+      if ((threadIdx.x & 31) == 0) raise_error(s.sync, MSB_ERR_TIMEOUT, task);
+      return false;
+    }
+  }
+}
+
+// Per-step header written by the producer into each stage.
+struct StepHdr {
+  int task, s, oct, gp;
+  int x0, x1, y0, y1, z0, z1;
+  int flags, mat;  // mat: which matrix buffer holds this task's octant
+  int stop, pad0, pad1, pad2;
+};
+
+template <int NM_, int NCH, int TX, int TY, int NS>
+struct Fp64Cfg {
+  static constexpr int KS = NM_ / 4;        // k-steps of the first product
+  static constexpr int MT = (NM_ + 7) / 8;  // m-tiles of the second product
+  static constexpr int NW = TX * TY;        // compute warps
+  static constexpr int NT = (NW + 4) * 32;  // threads: compute warps + one producer warpgroup
+  // With 8 compute warps the launch gives every thread 65536 / 384 = 168
+  // registers; the producer warpgroup hands most of its share to them.
+  static constexpr bool REBALANCE = NW == 8;
+  static constexpr int REG_PRODUCER = 96;
+  static constexpr int REG_COMPUTE = 200;  // 8*32*200 + 4*32*96 <= 384 * 168
+  static constexpr int ENT = NCH * 256;     // doubles per face entry
+  static constexpr bool FACE_PF = NCH == 1; // faces entering the tile staged by the producer
+  static constexpr int NXY = TX < TY ? TX : TY;
+  static constexpr int VSZ = 2 * NM_ * NU;  // doubles of vi (or vo) per warp-cell
+  // stage layout in doubles
+  static constexpr int ST_VI = 0;
+  static constexpr int ST_VO = ST_VI + NW * VSZ;
+  static constexpr int ST_YZ = ST_VO + NW * VSZ;
+  static constexpr int ST_XZ = ST_YZ + (FACE_PF ? TY * ENT : 0);
+  static constexpr int ST_XY = ST_XZ + (FACE_PF ? TX * ENT : 0);
+  static constexpr int ST_HDR = ST_XY + (FACE_PF ? NXY * ENT : 0);
+  static constexpr int STAGE = ST_HDR + (int)(sizeof(StepHdr) / sizeof(double));
+  static constexpr int MAT = NCH * (KS * 4 + MT * 8) * 32;  // doubles per matrix buffer
+  // smem layout in doubles
+  static constexpr int SM_SLOT = 0;                   // [2 faces][2 parity][NW][ENT]
+  static constexpr int SM_STAGE = 4 * NW * ENT;
+  static constexpr int SM_MAT = SM_STAGE + NS * STAGE;  // [2][MAT]
+  static constexpr int SM_BAR = SM_MAT + 2 * MAT;       // full[NS], done[NS]
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(SM_BAR + 2 * NS); }
+};
+
+template <int NM_, int NCH, int TX, int TY, int NS>
+__global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const Fp64Params P) {
+  using C = Fp64Cfg<NM_, NCH, TX, TY, NS>;
+  constexpr int KS = C::KS, MT = C::MT, NW = C::NW, ENT = C::ENT, VSZ = C::VSZ;
+  static_assert(NM_ % 4 == 0 && NM_ <= 16, "NM must be 4, 8 or 16");
+
+  extern __shared__ __align__(128) double smem[];
+  double* const slots = smem + C::SM_SLOT;
+  double* const stages = smem + C::SM_STAGE;
+  double* const mats = smem + C::SM_MAT;
+  uint64_t* const full = reinterpret_cast<uint64_t*>(smem + C::SM_BAR);
+  uint64_t* const done = full + NS;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int* const sync = P.sy.sync;
+  int* const progress = sync + SY_PROGRESS;
+  const size_t slab = (size_t)NM_ * NU * P.nx * P.ny;  // one (iz, ie) layer of the state
+  // loader <-> publisher hand-off (shared memory)
+  __shared__ volatile int s_pub_upto;   // steps whose done phase the publisher consumed
+  __shared__ volatile int s_final;      // total steps issued, once the loader stops (-1 before)
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(&full[i], 33);  // 32 loader lanes' cp.async arrivals + the header
+      mbar_init(&done[i], NW);
+    }
+    s_pub_upto = 0;
+    s_final = -1;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp >= NW) {
+    // ====================================================== producer warpgroup
+    if constexpr (C::REBALANCE) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(C::REG_PRODUCER));
+    if (warp == NW) {
+      // ------------------------------------------------------------ loader
+      long long g_load = 0;
+      long long last_step[2] = {-1, -1};  // last global step of the task using mat buffer 0/1
+      int ntask_seen = 0;
+      bool failed = false;
+
+      // bounded spin on the publisher's consumption counter
+      auto wait_pub = [&](long long until) -> bool {
+        if (s_pub_upto >= until) return true;
+        const long long t0 = global_ns();
+        while (s_pub_upto < until) {
+          __nanosleep(32);
+          if (global_ns() - t0 > P.sy.timeout_ns) {
+            if (lane == 0) raise_error(sync, MSB_ERR_TIMEOUT, -1);
+            return false;
+          }
+        }
+        return true;
+      };
+      // bounded wait for *p >= target; returns the value seen (or -1)
+      auto wait_dep = [&](const int* p, int target, int task) -> int {
+        int v = ld_acquire(p);
+        if (v >= target) return v;
+        const long long t0 = global_ns();
+        for (;;) {
+          __nanosleep(64);
+          v = ld_acquire(p);
+          if (v >= target) return v;
+          if (ld_relaxed(&sync[SY_ABORT]) != 0) return -1;
+          if (global_ns() - t0 > P.sy.timeout_ns) {
+            if (lane == 0) raise_error(sync, MSB_ERR_TIMEOUT, task);
+            return -1;
+          }
+        }
+      };
+      auto grab = [&]() -> int {
+        int t = -1;
+        if (lane == 0 && ld_relaxed(&sync[SY_ABORT]) == 0) {
+          const long long tt = atomicAdd(&sync[SY_COUNTER], 1);
+          t = tt < P.ntask ? (int)tt : -1;
+        }
+        return __shfl_sync(0xffffffffu, t, 0);
+      };
+
+      // A task is grabbed only once the previous one is fully issued (the
+      // compute warps still have NS steps of work in hand), so a reserved
+      // task never waits behind another task of the same CTA.
+      for (;;) {
+        const int t = grab();
+        if (t < 0) break;
+        const int rec_lane = lane < MSB_TASK_INTS ? __ldg(&P.tasks[(size_t)t * MSB_TASK_INTS + lane]) : 0;
+        int rec[MSB_TASK_INTS];
+#pragma unroll
+        for (int k = 0; k < MSB_TASK_INTS; ++k) rec[k] = __shfl_sync(0xffffffffu, rec_lane, k);
+
+        const int oct = rec[TK_OCT], gp = rec[TK_GP], flags = rec[TK_FLAGS], mode = rec[TK_DEP_MODE];
+        const int x0 = rec[TK_X0], x1 = rec[TK_X1], y0 = rec[TK_Y0], y1 = rec[TK_Y1];
+        const int z0 = rec[TK_Z0], z1 = rec[TK_Z1];
+        const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2;
+        const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
+        const int depx = (mode & DM_X_PLANE) ? rec[TK_DEP_X] : -1;
+        const int depy = (mode & DM_Y_PLANE) ? rec[TK_DEP_Y] : -1;
+        // cross-phase dependencies: whole task complete
+        if (rec[TK_DEP_X] >= 0 && depx < 0 && wait_dep(&progress[rec[TK_DEP_X]], kComplete, t) < 0) failed = true;
+        if (!failed && rec[TK_DEP_Y] >= 0 && depy < 0 && wait_dep(&progress[rec[TK_DEP_Y]], kComplete, t) < 0) failed = true;
+        if (!failed && rec[TK_DEP_Z] >= 0 && wait_dep(&progress[rec[TK_DEP_Z]], kComplete, t) < 0) failed = true;
+        if (!failed && rec[TK_DEP_VO] >= 0 && wait_dep(&progress[rec[TK_DEP_VO]], kComplete, t) < 0) failed = true;
+        // octant matrices into the buffer the task before last used
+        const int mb = ntask_seen & 1;
+        if (!failed && !wait_pub(last_step[mb] + 1)) failed = true;
+        if (failed) break;
+        __threadfence_block();
+        double* mat = mats + mb * C::MAT;
+        for (int e = lane; e < NCH * KS * 4 * 32; e += 32) {
+          const int ln = e & 31, tt = (e >> 5) & 3, k = (e >> 7) % KS, ch = (e >> 7) / KS;
+          const int ia = 32 * ch + 8 * tt + (ln >> 2), im = KS * (ln & 3) + k;
+          mat[e] = ia < P.na ? __ldg(&P.afm[ia + (size_t)P.na * (im + (size_t)NM_ * oct)]) : 0.0;
+        }
+        for (int e = lane; e < NCH * MT * 8 * 32; e += 32) {
+          const int ln = e & 31, i = (e >> 5) & 1, tt = (e >> 6) & 3, mt = (e >> 8) % MT, ch = (e >> 8) / MT;
+          const int ia = 32 * ch + 8 * tt + 2 * (ln & 3) + i, im = 8 * mt + (ln >> 2);
+          mat[NCH * KS * 4 * 32 + e] =
+              (ia < P.na && im < NM_) ? __ldg(&P.mfa[im + (size_t)NM_ * (ia + (size_t)P.na * oct)]) : 0.0;
+        }
+        __syncwarp();
+        ++ntask_seen;
+        last_step[mb] = g_load + nsteps - 1;
+
+        const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
+        const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;
+        int seen_x = 0, seen_y = 0;  // progress of the upwind tiles already observed
+        for (int s = 0; s < nsteps; ++s) {
+          const int st = (int)(g_load % NS);
+          // the stage was last used by step g_load - NS
+          if (g_load >= NS && !wait_pub(g_load - NS + 1)) { failed = true; break; }
+          // faces of this plane from the upwind tiles of the same phase
+          const int need = min(s + 1, nzr);
+          if (depx >= 0 && seen_x < need && (seen_x = wait_dep(&progress[depx], need, t)) < 0) { failed = true; break; }
+          if (depy >= 0 && seen_y < need && (seen_y = wait_dep(&progress[depy], need, t)) < 0) { failed = true; break; }
+          __threadfence_block();
+          double* stg = stages + (size_t)st * C::STAGE;
+          StepHdr* hdr = reinterpret_cast<StepHdr*>(stg + C::ST_HDR);
+          // Each lane copies 16-byte pieces of every segment (a 512-byte vi
+          // or vo block is one piece per lane); the lanes' cp.async arrivals
+          // complete the stage once all pieces have landed.
+          auto seg = [&](double* dst, const double* src, int bytes) {
+            for (int off = lane * 16; off < bytes; off += 32 * 16) cp_async16(dst + off / 8, src + off / 8);
+          };
+#pragma unroll 1
+          for (int wv = 0; wv < NW; ++wv) {
+            const int a = wv % TX, b = wv / TX, c = s - a - b;
+            if (a >= w || b >= h || c < 0 || c >= nzr) continue;
+            const int ix = dx > 0 ? x0 + a : x1 - 1 - a;
+            const int iy = dy > 0 ? y0 + b : y1 - 1 - b;
+            const int iz = dz > 0 ? z0 + c : z1 - 1 - c;
+            const size_t cb = (size_t)NM_ * NU * (ix + (size_t)P.nx * iy);
+#pragma unroll
+            for (int g2 = 0; g2 < 2; ++g2) {
+              const int g = 2 * gp + g2;
+              if (g >= P.ne) continue;
+              const size_t off = cb + slab * (g + (size_t)P.ne * iz);
+              seg(stg + C::ST_VI + wv * VSZ + g2 * (VSZ / 2), P.vi + off, VSZ / 2 * 8);
+              if (!(flags & TF_FIRST)) seg(stg + C::ST_VO + wv * VSZ + g2 * (VSZ / 2), P.vo + off, VSZ / 2 * 8);
+            }
+            if constexpr (C::FACE_PF) {
+              if (a == 0 && (flags & TF_X_IN))
+                seg(stg + C::ST_YZ + b * ENT, P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT, ENT * 8);
+              if (b == 0 && (flags & TF_Y_IN))
+                seg(stg + C::ST_XZ + a * ENT, P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT, ENT * 8);
+              if (c == 0 && (flags & TF_Z_IN))
+                seg(stg + C::ST_XY + b * ENT, P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT, ENT * 8);
+            }
+          }
+          cp_async_arrive_noinc(&full[st]);
+          if (lane == 0) {
+            hdr->task = t; hdr->s = s; hdr->oct = oct; hdr->gp = gp;
+            hdr->x0 = x0; hdr->x1 = x1; hdr->y0 = y0; hdr->y1 = y1; hdr->z0 = z0; hdr->z1 = z1;
+            hdr->flags = flags; hdr->mat = mb; hdr->stop = 0;
+            // progress this task reaches once step s is done (-2: nothing new)
+            hdr->pad0 = s == nsteps - 1 ? kComplete : (s + 1 - (w + h - 2) > 0 ? s + 1 - (w + h - 2) : -2);
+            mbar_arrive(&full[st]);
+          }
+          ++g_load;
+        }
+        if (failed) break;
+      }
+      // Drain: every stage that was issued is consumed by the compute warps
+      // (its copies always land); then a stop header ends their loop and the
+      // publisher stops at the same step.  A failed wait (error already
+      // recorded) ends the same way, so nothing in this CTA is left waiting.
+      if (lane == 0) s_final = (int)g_load;
+      if (wait_pub(g_load)) {
+        const int st = (int)(g_load % NS);  // last used by step g_load - NS, consumed
+        __threadfence_block();
+        cp_async_arrive_noinc(&full[st]);
+        if (lane == 0) {
+          StepHdr* hdr = reinterpret_cast<StepHdr*>(stages + (size_t)st * C::STAGE + C::ST_HDR);
+          hdr->stop = 1;
+          mbar_arrive(&full[st]);
+        }
+      }
+      __syncwarp();
+    } else if (warp == NW + 1) {
+      // --------------------------------------------------------- publisher
+      // Consumes the done phases in order and publishes this CTA's task
+      // progress, one fence per batch of finished steps.
+      long long G = 0;
+      long long t0 = global_ns();
+      for (;;) {
+        int pend_task[2] = {-1, -1}, pend_val[2] = {-2, -2};
+        bool advanced = false;
+        for (;;) {
+          const int fin = s_final;
+          if (fin >= 0 && G >= fin) break;
+          const int st = (int)(G % NS);
+          if (!mbar_test(&done[st], (uint32_t)((G / NS) & 1))) break;
+          const StepHdr* hdr = reinterpret_cast<const StepHdr*>(stages + (size_t)st * C::STAGE + C::ST_HDR);
+          const int task = hdr->task, val = hdr->pad0;
+          if (val != -2) {
+            if (pend_task[1] >= 0 && pend_task[1] != task) {
+              pend_task[0] = pend_task[1];
+              pend_val[0] = pend_val[1];
+            }
+            pend_task[1] = task;
+            pend_val[1] = val;
+          }
+          ++G;
+          __threadfence_block();
+          if (lane == 0) s_pub_upto = (int)G;
+          advanced = true;
+          // a task boundary ends a batch so older tasks are published first
+          if (pend_task[0] >= 0) break;
+        }
+        if (pend_task[1] >= 0 || pend_task[0] >= 0) {
+          __threadfence();
+          if (lane == 0) {
+            if (pend_task[0] >= 0) st_release(&progress[pend_task[0]], pend_val[0]);
+            if (pend_task[1] >= 0) st_release(&progress[pend_task[1]], pend_val[1]);
+          }
+        }
+        const int fin = s_final;
+        if (fin >= 0 && G >= fin) break;
+        if (advanced) {
+          t0 = global_ns();
+        } else {
+          __nanosleep(32);
+          if (global_ns() - t0 > P.sy.timeout_ns) {
+            if (lane == 0) raise_error(sync, MSB_ERR_TIMEOUT, -1);
+            break;
+          }
+        }
+      }
+    }
+    return;
+  }
+  if constexpr (C::REBALANCE) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(C::REG_COMPUTE));
+
+  // ================================================================ compute
+  const int q = lane >> 2, r = lane & 3;
+  const int wa = warp % TX, wb = warp / TX;
+  double wz[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) wz[i] = 1.0 / 4.0 - 1.0 / (double)(1 << (2 * r + i));
+
+  double b1r[NCH == 1 ? KS : 1][4];
+  double a2r[NCH == 1 ? MT : 1][4][2];
+  double carry[NCH][4][2];
+  int cur_task = -1;
+
+  for (long long G = 0;; ++G) {
+    const int st = (int)(G % NS);
+    if (!mbar_wait(&full[st], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
+    const double* stg = stages + (size_t)st * C::STAGE;
+    const StepHdr* hdr = reinterpret_cast<const StepHdr*>(stg + C::ST_HDR);
+    if (hdr->stop) break;
+    const int task = hdr->task, s = hdr->s, oct = hdr->oct, gp = hdr->gp, flags = hdr->flags;
+    const int x0 = hdr->x0, x1 = hdr->x1, y0 = hdr->y0, y1 = hdr->y1, z0 = hdr->z0, z1 = hdr->z1;
+    const double* mat = mats + hdr->mat * C::MAT;
+    const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0;
+    const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
+    if constexpr (NCH == 1) {
+      if (task != cur_task) {
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+#pragma unroll
+          for (int t = 0; t < 4; ++t) b1r[k][t] = mat[(k * 4 + t) * 32 + lane];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+          for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) a2r[mt][t][i] = mat[KS * 4 * 32 + ((mt * 4 + t) * 2 + i) * 32 + lane];
+      }
+    }
+    cur_task = task;
+
+    const int c = s - wa - wb;
+    if (wa < w && wb < h && c >= 0 && c < nzr) {
+      const int ix = dx > 0 ? x0 + wa : x1 - 1 - wa;
+      const int iy = dy > 0 ? y0 + wb : y1 - 1 - wb;
+      const int iz = dz > 0 ? z0 + c : z1 - 1 - c;
+      const int g_col = 2 * gp + (q >> 2), u_col = q & 3;
+      const bool gval = g_col < P.ne;
+      const int g_vo = 2 * gp + (r >> 1);
+      const bool first = (flags & TF_FIRST) != 0;
+
+      // vi fragments from the stage (zero for a missing second group)
+      double vif[KS];
+      {
+        const double* src = stg + C::ST_VI + warp * VSZ + (q >> 2) * (VSZ / 2) + NM_ * u_col + KS * r;
+#pragma unroll
+        for (int k = 0; k < KS; ++k) vif[k] = gval ? src[k] : 0.0;
+      }
+
+      const double so = (double)(1 + oct);
+      const double so_r = 1.0 / so;
+      const double s_sp = (double)d_scale_space(ix, iy, iz);
+      const double cxy = 0.5 / (double)d_scale_space(ix, iy, iz - dz);
+      const double cxz = 0.25 / (double)d_scale_space(ix, iy - dy, iz);
+      const double sx_r = 1.0 / (double)d_scale_space(ix - dx, iy, iz);
+      const double cyz[2] = {wz[0] * sx_r, wz[1] * sx_r};
+      const double cc = so_r * s_sp;
+
+      const int prev = (int)((G - 1) & 1), cur = (int)(G & 1);
+      double* const slot_yz = slots;                  // [2][NW][ENT]
+      double* const slot_xz = slots + 2 * NW * ENT;   // [2][NW][ENT]
+      // where the three incoming faces come from
+      const double* in_yz = nullptr;  // smem (neighbour warp or stage) ...
+      const double* gin_yz = nullptr; // ... or global (NCH > 1 edge warps)
+      const double* in_xz = nullptr;
+      const double* gin_xz = nullptr;
+      const double* in_xy = nullptr;
+      const double* gin_xy = nullptr;
+      const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
+      const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;
+      if (wa > 0) in_yz = slot_yz + (size_t)(prev * NW + warp - 1) * ENT;
+      else if (flags & TF_X_IN) {
+        if constexpr (C::FACE_PF) in_yz = stg + C::ST_YZ + wb * ENT;
+        else gin_yz = P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT;
+      }
+      if (wb > 0) in_xz = slot_xz + (size_t)(prev * NW + warp - TX) * ENT;
+      else if (flags & TF_Y_IN) {
+        if constexpr (C::FACE_PF) in_xz = stg + C::ST_XZ + wa * ENT;
+        else gin_xz = P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT;
+      }
+      if (c == 0 && (flags & TF_Z_IN)) {
+        if constexpr (C::FACE_PF) in_xy = stg + C::ST_XY + wb * ENT;
+        else gin_xy = P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT;
+      }
+      double* out_yz = slot_yz + (size_t)(cur * NW + warp) * ENT;
+      double* out_xz = slot_xz + (size_t)(cur * NW + warp) * ENT;
+      double* gout_yz = (wa == w - 1 && (flags & TF_X_OUT)) ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT : nullptr;
+      double* gout_xz = (wb == h - 1 && (flags & TF_Y_OUT)) ? P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT : nullptr;
+      double* gout_xy = (c == nzr - 1 && (flags & TF_Z_OUT)) ? P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT : nullptr;
+
+      double d2[MT][2][2];  // two accumulators per m-tile (even / odd t)
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) d2[mt][0][0] = d2[mt][0][1] = d2[mt][1][0] = d2[mt][1][1] = 0.0;
+
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        // ---- moments -> angles
+        double d1[4][2];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) d1[t][0] = d1[t][1] = 0.0;
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            const double b = NCH == 1 ? b1r[NCH == 1 ? k : 0][t] : mat[((ch * KS + k) * 4 + t) * 32 + lane];
+            dmma(d1[t], vif[k], b);
+          }
+
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const size_t eo = (size_t)((ch * 4 + t) * 32 + lane) * 2;
+          double fyz[2], fxz[2], fxy[2];
+          if (in_yz) {
+            const double2 v = *reinterpret_cast<const double2*>(in_yz + eo);
+            fyz[0] = v.x; fyz[1] = v.y;
+          } else if (gin_yz) {
+            const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_yz + eo));
+            fyz[0] = v.x; fyz[1] = v.y;
+          } else {
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int ia = 32 * ch + 8 * t + 2 * r + i;
+              fyz[i] = (gval && ia < P.na) ? d_init_face(ia, dx > 0 ? -1 : P.nx, iy, iz, g_col, u_col, oct) : 0.0;
+            }
+          }
+          if (in_xz) {
+            const double2 v = *reinterpret_cast<const double2*>(in_xz + eo);
+            fxz[0] = v.x; fxz[1] = v.y;
+          } else if (gin_xz) {
+            const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_xz + eo));
+            fxz[0] = v.x; fxz[1] = v.y;
+          } else {
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int ia = 32 * ch + 8 * t + 2 * r + i;
+              fxz[i] = (gval && ia < P.na) ? d_init_face(ia, ix, dy > 0 ? -1 : P.ny, iz, g_col, u_col, oct) : 0.0;
+            }
+          }
+          if (c > 0) {
+            fxy[0] = carry[ch][t][0]; fxy[1] = carry[ch][t][1];
+          } else if (in_xy) {
+            const double2 v = *reinterpret_cast<const double2*>(in_xy + eo);
+            fxy[0] = v.x; fxy[1] = v.y;
+          } else if (gin_xy) {
+            const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_xy + eo));
+            fxy[0] = v.x; fxy[1] = v.y;
+          } else {
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              const int ia = 32 * ch + 8 * t + 2 * r + i;
+              fxy[i] = (gval && ia < P.na) ? d_init_face(ia, ix, iy, dz > 0 ? -1 : P.nz, g_col, u_col, oct) : 0.0;
+            }
+          }
+
+          // ---- Quantities_solve, exact 7-operation form (no contraction)
+          double out[2];
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const double bxz = __dmul_rn(fxz[i], cxz);
+            const double sab = __fma_rn(fxy[i], cxy, bxz);  // fxy*cxy is exact
+            const double cyzv = __dmul_rn(fyz[i], cyz[i]);
+            const double sm = __dadd_rn(sab, cyzv);
+            const double psi = __dadd_rn(d1[t][i], __dmul_rn(sm, cc));
+            d1[t][i] = psi;
+            out[i] = __dmul_rn(psi, so);
+            carry[ch][t][i] = out[i];
+          }
+          const double2 ov = make_double2(out[0], out[1]);
+          *reinterpret_cast<double2*>(out_yz + eo) = ov;
+          *reinterpret_cast<double2*>(out_xz + eo) = ov;
+          if (gout_yz) __stcg(reinterpret_cast<double2*>(gout_yz + eo), ov);
+          if (gout_xz) __stcg(reinterpret_cast<double2*>(gout_xz + eo), ov);
+          if (gout_xy) __stcg(reinterpret_cast<double2*>(gout_xy + eo), ov);
+
+          // ---- angles -> moments for this t (psi is the B operand as is)
+#pragma unroll
+          for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+              const double a = NCH == 1 ? a2r[NCH == 1 ? mt : 0][t][i]
+                                        : mat[NCH * KS * 4 * 32 + ((((ch * MT + mt) * 4 + t) * 2 + i) * 32) + lane];
+              dmma(d2[mt][t & 1], a, d1[t][i]);
+            }
+        }
+      }
+
+      // ---- accumulate vo in the region's visiting order
+      if (g_vo < P.ne) {
+        const size_t vbase = (size_t)NM_ * NU * (ix + (size_t)P.nx * iy) + slab * (g_vo + (size_t)P.ne * iz);
+        const double* vold = stg + C::ST_VO + warp * VSZ + (r >> 1) * (VSZ / 2);
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int im = 8 * mt + q;
+            if (im < NM_) {
+              const int o = NM_ * (2 * (r & 1) + j) + im;
+              const double dsum = __dadd_rn(d2[mt][0][j], d2[mt][1][j]);
+              P.vo[vbase + o] = first ? dsum : __dadd_rn(vold[o], dsum);
+            }
+          }
+      }
+    }
+    // step G done by this warp: its writes are ordered before the arrive;
+    // once every compute warp has arrived, the neighbours' faces of step G
+    // are visible and step G + 1 may start
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&done[st]);
+    if (!mbar_wait(&done[st], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
+  }
+}
+
+}  // namespace msb

@@ -12,7 +12,7 @@
 #include <new>
 
 #include "internal.h"
-#include "sweep_fp64.cuh"
+#include "sweep_fp64_ws.cuh"
 
 namespace msb {
 
@@ -23,17 +23,22 @@ using KernelFn = void (*)(const Fp64Params);
 struct Variant {
   KernelFn fn = nullptr;
   size_t smem = 0;
-  int tx = 0, ty = 0, nch = 0;
+  int tx = 0, ty = 0, nch = 0, threads = 0;
 };
+
+constexpr int kStages = 4;
 
 template <int NM_, int NCH, int TX, int TY>
 Variant make_variant() {
+  using C = Fp64Cfg<NM_, NCH, TX, TY, kStages>;
+  static_assert(C::smem_bytes() <= 227 * 1024, "shared memory budget");
   Variant v;
-  v.fn = sweep_fp64_kernel<NM_, NCH, TX, TY>;
-  v.smem = Fp64Cfg<NM_, NCH, TX, TY>::smem_bytes();
+  v.fn = sweep_fp64_kernel<NM_, NCH, TX, TY, kStages>;
+  v.smem = C::smem_bytes();
   v.tx = TX;
   v.ty = TY;
   v.nch = NCH;
+  v.threads = C::NT;
   return v;
 }
 
@@ -65,6 +70,7 @@ constexpr long long kDefaultTimeoutNs = 4000000000LL;  // 4 s per wait
 struct SweeperImpl {
   Dimensions dims{};
   int ngp = 0;
+  int gp_block = 1;
   Variant var;
   Schedule sched;
   int grid = 0;
@@ -102,7 +108,11 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims) {
     return set_error(MSB_ERR_UNSUPPORTED, "no kernel variant for nm=%d na=%d (nm in {4,8,16}, na <= 128)",
                      dims.nm, dims.na);
   S.ngp = (dims.ne + 1) / 2;
-  int rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, S.var.tx, S.var.ty, S.sched);
+  int rc, dev = 0, nsm = 0, occ = 0;
+  if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+  if ((rc = cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rc;
+  S.gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, S.var.tx, S.var.ty, 2 * nsm);
+  rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, S.var.tx, S.var.ty, S.gp_block, S.sched);
   if (rc) return rc;
   const long long ntask = S.sched.ntask();
   if (ntask >= (1LL << 31) - SY_PROGRESS) return set_error(MSB_ERR_ARG, "too many tasks");
@@ -130,10 +140,7 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims) {
   if ((rc = cuda_check(cudaFuncSetAttribute(S.var.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S.var.smem),
                        "cudaFuncSetAttribute")))
     return rc;
-  int dev = 0, nsm = 0, occ = 0;
-  if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
-  if ((rc = cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rc;
-  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, S.var.fn, S.var.tx * S.var.ty * 32,
+  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, S.var.fn, S.var.threads,
                                                                      S.var.smem),
                        "occupancy")))
     return rc;
@@ -181,7 +188,7 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
   P.ngp = S.ngp;
   P.sy.sync = S.d_sync;
   P.sy.timeout_ns = S.timeout_ns;
-  S.var.fn<<<S.grid, S.var.tx * S.var.ty * 32, S.var.smem, stream>>>(P);
+  S.var.fn<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
   if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
                        "status copy")))

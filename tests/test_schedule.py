@@ -30,9 +30,9 @@ SIZES = [(1, 1, 1, 1), (2, 1, 2, 3), (5, 4, 5, 3), (3, 4, 2, 5), (7, 5, 3, 2), (
 
 
 @pytest.mark.parametrize("nx,ny,nz,ne", SIZES)
-@pytest.mark.parametrize("tx,ty", [(4, 2), (2, 2)])
-def test_schedule_properties(nx, ny, nz, ne, tx, ty):
-    T = msb.schedule(nx, ny, nz, ne, tx, ty)
+@pytest.mark.parametrize("tx,ty,gpb", [(4, 2, 1), (2, 2, 1), (4, 2, 2), (4, 2, 3)])
+def test_schedule_properties(nx, ny, nz, ne, tx, ty, gpb):
+    T = msb.schedule(nx, ny, nz, ne, tx, ty, gpb)
     ngp = (ne + 1) // 2
     own = cell_owner(T, nx, ny, nz, ngp)
     assert (own >= 0).all(), "cell not swept"
