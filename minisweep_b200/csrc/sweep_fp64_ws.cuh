@@ -96,14 +96,21 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// 16-byte asynchronous copy global -> shared (L2 only), and the arrival on an
-// mbarrier once all of this thread's earlier cp.async copies have landed.
+// 16-byte asynchronous copy global -> shared (L2 only) and its groups.
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// 1-D bulk copy global -> shared, completion counted on an mbarrier.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
 // Bounded wait on an mbarrier phase by a whole warp (all lanes poll).  It
 // does not give up when another CTA aborts: inside a CTA every phase that was
@@ -142,7 +149,7 @@ struct Fp64Cfg {
   static constexpr int REG_COMPUTE = 200;  // 8*32*200 + 4*32*96 <= 384 * 168
   static constexpr int ENT = NCH * 256;     // doubles per face entry
   static constexpr bool FACE_PF = NCH == 1; // faces entering the tile staged by the producer
-  static constexpr int NXY = TX < TY ? TX : TY;
+  static constexpr int NXY = TY;  // first-plane xy faces staged per step: one per row
   static constexpr int VSZ = 2 * NM_ * NU;  // doubles of vi (or vo) per warp-cell
   // stage layout in doubles
   static constexpr int ST_VI = 0;
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < NS; ++i) {
-      mbar_init(&full[i], 33);  // 32 loader lanes' cp.async arrivals + the header
+      mbar_init(&full[i], 1);  // the loader's arrive.expect_tx (header + face copies)
       mbar_init(&done[i], NW);
     }
     s_pub_upto = 0;
@@ -296,48 +303,58 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
           const int need = min(s + 1, nzr);
           if (depx >= 0 && seen_x < need && (seen_x = wait_dep(&progress[depx], need, t)) < 0) { failed = true; break; }
           if (depy >= 0 && seen_y < need && (seen_y = wait_dep(&progress[depy], need, t)) < 0) { failed = true; break; }
+          fence_proxy_async();
           __threadfence_block();
           double* stg = stages + (size_t)st * C::STAGE;
           StepHdr* hdr = reinterpret_cast<StepHdr*>(stg + C::ST_HDR);
-          // Each lane copies 16-byte pieces of every segment (a 512-byte vi
-          // or vo block is one piece per lane); the lanes' cp.async arrivals
-          // complete the stage once all pieces have landed.
-          auto seg = [&](double* dst, const double* src, int bytes) {
-            for (int off = lane * 16; off < bytes; off += 32 * 16) cp_async16(dst + off / 8, src + off / 8);
-          };
-#pragma unroll 1
-          for (int wv = 0; wv < NW; ++wv) {
-            const int a = wv % TX, b = wv / TX, c = s - a - b;
-            if (a >= w || b >= h || c < 0 || c >= nzr) continue;
-            const int ix = dx > 0 ? x0 + a : x1 - 1 - a;
-            const int iy = dy > 0 ? y0 + b : y1 - 1 - b;
-            const int iz = dz > 0 ? z0 + c : z1 - 1 - c;
-            const size_t cb = (size_t)NM_ * NU * (ix + (size_t)P.nx * iy);
-#pragma unroll
-            for (int g2 = 0; g2 < 2; ++g2) {
-              const int g = 2 * gp + g2;
-              if (g >= P.ne) continue;
-              const size_t off = cb + slab * (g + (size_t)P.ne * iz);
-              seg(stg + C::ST_VI + wv * VSZ + g2 * (VSZ / 2), P.vi + off, VSZ / 2 * 8);
-              if (!(flags & TF_FIRST)) seg(stg + C::ST_VO + wv * VSZ + g2 * (VSZ / 2), P.vo + off, VSZ / 2 * 8);
+          // Faces entering the tile at this step, one bulk copy each: lane j
+          // handles piece j = (kind, position) with kind 0 yz (x-upwind edge,
+          // row b), 1 xz (y-upwind edge, column a), 2 xy (first plane of
+          // column (a, b) with b = row of the anti-diagonal cell).
+          uint32_t bytes = 0;
+          if constexpr (C::FACE_PF) {
+            for (int b = 0; b < h; ++b) {
+              const int c = s - b;
+              if ((flags & TF_X_IN) && c >= 0 && c < nzr) bytes += ENT * 8;
+              const int a = s - b;
+              if ((flags & TF_Z_IN) && a >= 0 && a < w) bytes += ENT * 8;
             }
-            if constexpr (C::FACE_PF) {
-              if (a == 0 && (flags & TF_X_IN))
-                seg(stg + C::ST_YZ + b * ENT, P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT, ENT * 8);
-              if (b == 0 && (flags & TF_Y_IN))
-                seg(stg + C::ST_XZ + a * ENT, P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT, ENT * 8);
-              if (c == 0 && (flags & TF_Z_IN))
-                seg(stg + C::ST_XY + b * ENT, P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT, ENT * 8);
+            for (int a = 0; a < w; ++a) {
+              const int c = s - a;
+              if ((flags & TF_Y_IN) && c >= 0 && c < nzr) bytes += ENT * 8;
             }
           }
-          cp_async_arrive_noinc(&full[st]);
           if (lane == 0) {
             hdr->task = t; hdr->s = s; hdr->oct = oct; hdr->gp = gp;
             hdr->x0 = x0; hdr->x1 = x1; hdr->y0 = y0; hdr->y1 = y1; hdr->z0 = z0; hdr->z1 = z1;
             hdr->flags = flags; hdr->mat = mb; hdr->stop = 0;
             // progress this task reaches once step s is done (-2: nothing new)
             hdr->pad0 = s == nsteps - 1 ? kComplete : (s + 1 - (w + h - 2) > 0 ? s + 1 - (w + h - 2) : -2);
-            mbar_arrive(&full[st]);
+            mbar_arrive_expect_tx(&full[st], bytes);
+          }
+          __syncwarp();
+          if constexpr (C::FACE_PF) {
+            // lanes [0, TY): yz of row b; [8, 8+TX): xz of column a; [16, 16+TY): xy of row b
+            const int kind = lane >> 3, pos = lane & 7;
+            if (kind == 0 && pos < h && (flags & TF_X_IN)) {
+              const int b = pos, c = s - b;
+              if (c >= 0 && c < nzr) {
+                const int iy = dy > 0 ? y0 + b : y1 - 1 - b, iz = dz > 0 ? z0 + c : z1 - 1 - c;
+                bulk_g2s(stg + C::ST_YZ + b * ENT, P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT, ENT * 8, &full[st]);
+              }
+            } else if (kind == 1 && pos < w && (flags & TF_Y_IN)) {
+              const int a = pos, c = s - a;
+              if (c >= 0 && c < nzr) {
+                const int ix = dx > 0 ? x0 + a : x1 - 1 - a, iz = dz > 0 ? z0 + c : z1 - 1 - c;
+                bulk_g2s(stg + C::ST_XZ + a * ENT, P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT, ENT * 8, &full[st]);
+              }
+            } else if (kind == 2 && pos < h && (flags & TF_Z_IN)) {
+              const int b = pos, a = s - b;
+              if (a >= 0 && a < w) {
+                const int ix = dx > 0 ? x0 + a : x1 - 1 - a, iy = dy > 0 ? y0 + b : y1 - 1 - b;
+                bulk_g2s(stg + C::ST_XY + b * ENT, P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT, ENT * 8, &full[st]);
+              }
+            }
           }
           ++g_load;
         }
@@ -351,11 +368,10 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       if (wait_pub(g_load)) {
         const int st = (int)(g_load % NS);  // last used by step g_load - NS, consumed
         __threadfence_block();
-        cp_async_arrive_noinc(&full[st]);
         if (lane == 0) {
           StepHdr* hdr = reinterpret_cast<StepHdr*>(stages + (size_t)st * C::STAGE + C::ST_HDR);
           hdr->stop = 1;
-          mbar_arrive(&full[st]);
+          mbar_arrive_expect_tx(&full[st], 0);
         }
       }
       __syncwarp();
@@ -451,7 +467,43 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
             for (int i = 0; i < 2; ++i) a2r[mt][t][i] = mat[KS * 4 * 32 + ((mt * 4 + t) * 2 + i) * 32 + lane];
       }
     }
+
+    // Each warp stages its own vi (and the previous vo) two steps ahead with
+    // 16-byte cp.async copies into the stage of that step; one commit group
+    // per step keeps the group count uniform.  A new task starts with the
+    // groups of its steps 0 and 1.
+    const int nsteps = nzr + w + h - 2;
+    const bool first = (flags & TF_FIRST) != 0;
+    auto prefetch = [&](int s2, long long G2) {
+      const int c2 = s2 - wa - wb;
+      if (s2 < nsteps && wa < w && wb < h && c2 >= 0 && c2 < nzr) {
+        const int ix2 = dx > 0 ? x0 + wa : x1 - 1 - wa;
+        const int iy2 = dy > 0 ? y0 + wb : y1 - 1 - wb;
+        const int iz2 = dz > 0 ? z0 + c2 : z1 - 1 - c2;
+        double* dst = stages + (size_t)(G2 % NS) * C::STAGE + warp * VSZ;
+        const size_t cb = (size_t)NM_ * NU * (ix2 + (size_t)P.nx * iy2);
+#pragma unroll
+        for (int g2 = 0; g2 < 2; ++g2) {
+          const int g = 2 * gp + g2;
+          if (g >= P.ne) continue;
+          const size_t off = cb + slab * (g + (size_t)P.ne * iz2);
+#pragma unroll
+          for (int o = lane * 2; o < VSZ / 2; o += 64) {
+            cp_async16(dst + C::ST_VI + g2 * (VSZ / 2) + o, P.vi + off + o);
+            if (!first) cp_async16(dst + C::ST_VO + g2 * (VSZ / 2) + o, P.vo + off + o);
+          }
+        }
+      }
+      cp_async_commit();
+    };
+    if (task != cur_task) {
+      prefetch(s, G);
+      prefetch(s + 1, G + 1);
+    }
+    prefetch(s + 2, G + 2);
     cur_task = task;
+    cp_async_wait<2>();  // this step's group has landed (this thread's copies)
+    __syncwarp();        // ... and every lane's
 
     const int c = s - wa - wb;
     if (wa < w && wb < h && c >= 0 && c < nzr) {
@@ -461,7 +513,6 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       const int g_col = 2 * gp + (q >> 2), u_col = q & 3;
       const bool gval = g_col < P.ne;
       const int g_vo = 2 * gp + (r >> 1);
-      const bool first = (flags & TF_FIRST) != 0;
 
       // vi fragments from the stage (zero for a missing second group)
       double vif[KS];
@@ -632,6 +683,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
     if (lane == 0) mbar_arrive(&done[st]);
     if (!mbar_wait(&done[st], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
   }
+  cp_async_wait<0>();  // no copy into shared memory outlives the CTA
 }
 
 }  // namespace msb
