@@ -76,6 +76,10 @@ static __device__ __noinline__ bool wait_geq(const SyncArgs& s, const int* p, in
 __device__ __forceinline__ int d_scale_space(int ix, int iy, int iz) {
   return 1 << ((ix + 3 * iy + 7 * iz + 2) & 3);
 }
+// log2 of the space scale factor, and 2^k / 2^-k built from exponent bits
+// (exact; used instead of FP64 divisions by the power-of-two factors).
+__device__ __forceinline__ int d_log2_space(int ix, int iy, int iz) { return (ix + 3 * iy + 7 * iz + 2) & 3; }
+__device__ __forceinline__ double d_pow2(int k) { return __longlong_as_double((long long)(1023 + k) << 52); }
 __device__ __forceinline__ int d_scale_energy(int ie) { return 1 << (((ie * 1366 + 150889) % 714025) & 3); }
 __device__ __forceinline__ int d_scale_unknown(int iu) { return 1 << (((iu * 741 + 66037) % 312500) & 3); }
 

@@ -112,15 +112,27 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
-// Bounded wait on an mbarrier phase by a whole warp (all lanes poll).  It
-// does not give up when another CTA aborts: inside a CTA every phase that was
-// started is completed (the producer finishes the stages it issued and then
-// posts a stop), so only a time-out ends it early.
+// try_wait with a suspend-time hint: the warp sleeps in hardware until the
+// phase completes or about `ns` nanoseconds pass (no busy polling).
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase by a whole warp.  It does not give up
+// when another CTA aborts: inside a CTA every phase that was started is
+// completed (the loader finishes the stages it issued and then posts a stop),
+// so only a time-out ends it early.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const SyncArgs& s, int task) {
-  if (mbar_test(b, parity)) return true;
+  if (mbar_try_wait(b, parity, 20000)) return true;
   const long long t0 = global_ns();
   for (;;) {
-    if (mbar_test(b, parity)) return true;
+    if (mbar_try_wait(b, parity, 100000)) return true;
     if (global_ns() - t0 > s.timeout_ns) {
       if ((threadIdx.x & 31) == 0) raise_error(s.sync, MSB_ERR_TIMEOUT, task);
       return false;
@@ -164,11 +176,11 @@ struct Fp64Cfg {
   static constexpr int SM_SLOT = 0;                   // [2 faces][2 parity][NW][ENT]
   static constexpr int SM_STAGE = 4 * NW * ENT;
   static constexpr int SM_MAT = SM_STAGE + NS * STAGE;  // [2][MAT]
-  static constexpr int SM_BAR = SM_MAT + 2 * MAT;       // full[NS], done[NS]
-  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(SM_BAR + 2 * NS); }
+  static constexpr int SM_BAR = SM_MAT + 2 * MAT;       // full[NS], done[NS], freed[NS]
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(SM_BAR + 3 * NS); }
 };
 
-template <int NM_, int NCH, int TX, int TY, int NS>
+template <int NM_, int NCH, int TX, int TY, int NS, bool PIPE_T1>
 __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const Fp64Params P) {
   using C = Fp64Cfg<NM_, NCH, TX, TY, NS>;
   constexpr int KS = C::KS, MT = C::MT, NW = C::NW, ENT = C::ENT, VSZ = C::VSZ;
@@ -180,21 +192,21 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
   double* const mats = smem + C::SM_MAT;
   uint64_t* const full = reinterpret_cast<uint64_t*>(smem + C::SM_BAR);
   uint64_t* const done = full + NS;
+  uint64_t* const freed = done + NS;  // publisher consumed the step: loader may refill the stage
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* const sync = P.sy.sync;
   int* const progress = sync + SY_PROGRESS;
   const size_t slab = (size_t)NM_ * NU * P.nx * P.ny;  // one (iz, ie) layer of the state
   // loader <-> publisher hand-off (shared memory)
-  __shared__ volatile int s_pub_upto;   // steps whose done phase the publisher consumed
   __shared__ volatile int s_final;      // total steps issued, once the loader stops (-1 before)
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < NS; ++i) {
       mbar_init(&full[i], 1);  // the loader's arrive.expect_tx (header + face copies)
       mbar_init(&done[i], NW);
+      mbar_init(&freed[i], 1);
     }
-    s_pub_upto = 0;
     s_final = -1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -210,16 +222,14 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       int ntask_seen = 0;
       bool failed = false;
 
-      // bounded spin on the publisher's consumption counter
-      auto wait_pub = [&](long long until) -> bool {
-        if (s_pub_upto >= until) return true;
-        const long long t0 = global_ns();
-        while (s_pub_upto < until) {
-          __nanosleep(32);
-          if (global_ns() - t0 > P.sy.timeout_ns) {
-            if (lane == 0) raise_error(sync, MSB_ERR_TIMEOUT, -1);
-            return false;
-          }
+      // Steps up to freed_upto have been consumed by the publisher.  Waiting
+      // for step g uses the phase of freed[g % NS] that step g completes;
+      // it is always that barrier's latest phase, so parities never alias.
+      long long freed_upto = -1;
+      auto wait_freed = [&](long long g) -> bool {
+        for (long long x = freed_upto + 1; x <= g; ++x) {
+          if (!mbar_wait(&freed[x % NS], (uint32_t)((x / NS) & 1), P.sy, -1)) return false;
+          freed_upto = x;
         }
         return true;
       };
@@ -273,7 +283,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
         if (!failed && rec[TK_DEP_VO] >= 0 && wait_dep(&progress[rec[TK_DEP_VO]], kComplete, t) < 0) failed = true;
         // octant matrices into the buffer the task before last used
         const int mb = ntask_seen & 1;
-        if (!failed && !wait_pub(last_step[mb] + 1)) failed = true;
+        if (!failed && !wait_freed(last_step[mb])) failed = true;
         if (failed) break;
         __threadfence_block();
         double* mat = mats + mb * C::MAT;
@@ -298,7 +308,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
         for (int s = 0; s < nsteps; ++s) {
           const int st = (int)(g_load % NS);
           // the stage was last used by step g_load - NS
-          if (g_load >= NS && !wait_pub(g_load - NS + 1)) { failed = true; break; }
+          if (g_load >= NS && !wait_freed(g_load - NS)) { failed = true; break; }
           // faces of this plane from the upwind tiles of the same phase
           const int need = min(s + 1, nzr);
           if (depx >= 0 && seen_x < need && (seen_x = wait_dep(&progress[depx], need, t)) < 0) { failed = true; break; }
@@ -365,7 +375,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       // publisher stops at the same step.  A failed wait (error already
       // recorded) ends the same way, so nothing in this CTA is left waiting.
       if (lane == 0) s_final = (int)g_load;
-      if (wait_pub(g_load)) {
+      if (wait_freed(g_load - 1)) {
         const int st = (int)(g_load % NS);  // last used by step g_load - NS, consumed
         __threadfence_block();
         if (lane == 0) {
@@ -377,20 +387,34 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       __syncwarp();
     } else if (warp == NW + 1) {
       // --------------------------------------------------------- publisher
-      // Consumes the done phases in order and publishes this CTA's task
-      // progress, one fence per batch of finished steps.
+      // Sleeps on the done phases in order, hands each stage back to the
+      // loader and publishes this CTA's task progress, one fence per batch
+      // of steps that finished together.
       long long G = 0;
       long long t0 = global_ns();
-      for (;;) {
-        int pend_task[2] = {-1, -1}, pend_val[2] = {-2, -2};
-        bool advanced = false;
+      bool quit = false;
+      while (!quit) {
+        // wait for step G (or for the loader to stop before it)
+        const int st0 = (int)(G % NS);
+        bool ready = false;
         for (;;) {
           const int fin = s_final;
-          if (fin >= 0 && G >= fin) break;
+          if (fin >= 0 && G >= fin) { quit = true; break; }
+          if (mbar_try_wait(&done[st0], (uint32_t)((G / NS) & 1), 2000)) { ready = true; break; }
+          if (global_ns() - t0 > P.sy.timeout_ns) {
+            if (lane == 0) raise_error(sync, MSB_ERR_TIMEOUT, -1);
+            quit = true;
+            break;
+          }
+        }
+        if (!ready) break;
+        int pend_task[2] = {-1, -1}, pend_val[2] = {-2, -2};
+        for (;;) {  // consume step G and any later steps already done
           const int st = (int)(G % NS);
-          if (!mbar_test(&done[st], (uint32_t)((G / NS) & 1))) break;
           const StepHdr* hdr = reinterpret_cast<const StepHdr*>(stages + (size_t)st * C::STAGE + C::ST_HDR);
           const int task = hdr->task, val = hdr->pad0;
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&freed[st]);
           if (val != -2) {
             if (pend_task[1] >= 0 && pend_task[1] != task) {
               pend_task[0] = pend_task[1];
@@ -400,11 +424,11 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
             pend_val[1] = val;
           }
           ++G;
-          __threadfence_block();
-          if (lane == 0) s_pub_upto = (int)G;
-          advanced = true;
           // a task boundary ends a batch so older tasks are published first
           if (pend_task[0] >= 0) break;
+          const int fin = s_final;
+          if (fin >= 0 && G >= fin) break;
+          if (!mbar_test(&done[G % NS], (uint32_t)((G / NS) & 1))) break;
         }
         if (pend_task[1] >= 0 || pend_task[0] >= 0) {
           __threadfence();
@@ -413,17 +437,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
             if (pend_task[1] >= 0) st_release(&progress[pend_task[1]], pend_val[1]);
           }
         }
-        const int fin = s_final;
-        if (fin >= 0 && G >= fin) break;
-        if (advanced) {
-          t0 = global_ns();
-        } else {
-          __nanosleep(32);
-          if (global_ns() - t0 > P.sy.timeout_ns) {
-            if (lane == 0) raise_error(sync, MSB_ERR_TIMEOUT, -1);
-            break;
-          }
-        }
+        t0 = global_ns();
       }
     }
     return;
@@ -436,252 +450,268 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
   double wz[2];
 #pragma unroll
   for (int i = 0; i < 2; ++i) wz[i] = 1.0 / 4.0 - 1.0 / (double)(1 << (2 * r + i));
+  double* const slot_yz = slots;                 // [2][NW][ENT]
+  double* const slot_xz = slots + 2 * NW * ENT;  // [2][NW][ENT]
+  // lane-constant offsets inside a warp's stage blocks and face entries
+  const int vi_lane = (q >> 2) * (VSZ / 2) + NM_ * (q & 3) + KS * r;  // vi fragment
+  const int vo_lane = (r >> 1) * (VSZ / 2) + NM_ * 2 * (r & 1) + q;   // vo value (mt = 0, j = 0)
 
   double b1r[NCH == 1 ? KS : 1][4];
   double a2r[NCH == 1 ? MT : 1][4][2];
   double carry[NCH][4][2];
-  int cur_task = -1;
+  double d1n[NCH][4][2];  // angle values of the next plane (PIPE_T1)
 
-  for (long long G = 0;; ++G) {
-    const int st = (int)(G % NS);
-    if (!mbar_wait(&full[st], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
-    const double* stg = stages + (size_t)st * C::STAGE;
-    const StepHdr* hdr = reinterpret_cast<const StepHdr*>(stg + C::ST_HDR);
-    if (hdr->stop) break;
-    const int task = hdr->task, s = hdr->s, oct = hdr->oct, gp = hdr->gp, flags = hdr->flags;
-    const int x0 = hdr->x0, x1 = hdr->x1, y0 = hdr->y0, y1 = hdr->y1, z0 = hdr->z0, z1 = hdr->z1;
-    const double* mat = mats + hdr->mat * C::MAT;
-    const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0;
+  long long G = 0;
+  for (;;) {
+    // ------------------------------------------------ one task per iteration
+    if (!mbar_wait(&full[G % NS], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
+    const StepHdr* hdr0 = reinterpret_cast<const StepHdr*>(stages + (size_t)(G % NS) * C::STAGE + C::ST_HDR);
+    if (hdr0->stop) break;
+    const int oct = hdr0->oct, gp = hdr0->gp, flags = hdr0->flags;
+    const int x0 = hdr0->x0, x1 = hdr0->x1, y0 = hdr0->y0, y1 = hdr0->y1, z0 = hdr0->z0, z1 = hdr0->z1;
+    const double* mat = mats + hdr0->mat * C::MAT;
+    const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2;
     const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
+    const bool first = (flags & TF_FIRST) != 0;
+    const bool act = wa < w && wb < h;
+    const int ix = dx > 0 ? x0 + wa : x1 - 1 - wa;
+    const int iy = dy > 0 ? y0 + wb : y1 - 1 - wb;
+    const int iz0 = dz > 0 ? z0 : z1 - 1;  // z of plane 0; plane c is iz0 + dz * c
+    const int cbeg = wa + wb;              // step of this warp's plane 0
+    const int g_col = 2 * gp + (q >> 2);
+    const bool gval = g_col < P.ne;
+    const int g_vo = 2 * gp + (r >> 1);
+    const bool gvo = g_vo < P.ne;
+    const double so = (double)(1 + oct);
+    const double so_r = 1.0 / so;  // rounded, as the reference's 1/(1+octant)
+    // boundary flux = (1+ia) 2^(ia&7) s_space s_energy s_unknown (1+oct):
+    // exact small integers, so the per-lane factor is formed once per task
+    const double face_k = gval ? (double)d_scale_energy(g_col) * (double)d_scale_unknown(q & 3) * so : 0.0;
+    const int sp_xy = ix + 3 * iy + 2;  // log2 s_space(x, y, z) = (sp_xy + 7 z) & 3
+    // state offsets (doubles) of this column: + zstep per plane
+    const size_t col = (size_t)NM_ * NU * (ix + (size_t)P.nx * iy);
+    const long long zstep = (long long)slab * P.ne * dz;
+    const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
+    const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;
+    // edges of the tile that read or write global faces
+    const bool x_in = wa == 0 && (flags & TF_X_IN), y_in = wb == 0 && (flags & TF_Y_IN);
+    const bool z_in = (flags & TF_Z_IN) != 0;
+    const bool x_out = wa == w - 1 && (flags & TF_X_OUT), y_out = wb == h - 1 && (flags & TF_Y_OUT);
+    const bool z_out = (flags & TF_Z_OUT) != 0;
     if constexpr (NCH == 1) {
-      if (task != cur_task) {
 #pragma unroll
-        for (int k = 0; k < KS; ++k)
+      for (int k = 0; k < KS; ++k)
 #pragma unroll
-          for (int t = 0; t < 4; ++t) b1r[k][t] = mat[(k * 4 + t) * 32 + lane];
+        for (int t = 0; t < 4; ++t) b1r[k][t] = mat[(k * 4 + t) * 32 + lane];
 #pragma unroll
-        for (int mt = 0; mt < MT; ++mt)
+      for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-          for (int t = 0; t < 4; ++t)
+        for (int t = 0; t < 4; ++t)
 #pragma unroll
-            for (int i = 0; i < 2; ++i) a2r[mt][t][i] = mat[KS * 4 * 32 + ((mt * 4 + t) * 2 + i) * 32 + lane];
-      }
+          for (int i = 0; i < 2; ++i) a2r[mt][t][i] = mat[KS * 4 * 32 + ((mt * 4 + t) * 2 + i) * 32 + lane];
     }
 
-    // Each warp stages its own vi (and the previous vo) two steps ahead with
-    // 16-byte cp.async copies into the stage of that step; one commit group
-    // per step keeps the group count uniform.  A new task starts with the
-    // groups of its steps 0 and 1.
-    const int nsteps = nzr + w + h - 2;
-    const bool first = (flags & TF_FIRST) != 0;
+    // Each warp stages its own vi (and the previous vo) three steps ahead
+    // with 16-byte cp.async copies into the stage of that step; one commit
+    // group per step keeps the group count uniform.
     auto prefetch = [&](int s2, long long G2) {
-      const int c2 = s2 - wa - wb;
-      if (s2 < nsteps && wa < w && wb < h && c2 >= 0 && c2 < nzr) {
-        const int ix2 = dx > 0 ? x0 + wa : x1 - 1 - wa;
-        const int iy2 = dy > 0 ? y0 + wb : y1 - 1 - wb;
-        const int iz2 = dz > 0 ? z0 + c2 : z1 - 1 - c2;
+      const int c2 = s2 - cbeg;
+      if (act && s2 < nsteps && c2 >= 0 && c2 < nzr) {
         double* dst = stages + (size_t)(G2 % NS) * C::STAGE + warp * VSZ;
-        const size_t cb = (size_t)NM_ * NU * (ix2 + (size_t)P.nx * iy2);
+        const size_t off0 = col + slab * (size_t)(2 * gp) + (size_t)(slab * P.ne) * (size_t)(iz0 + dz * c2);
 #pragma unroll
         for (int g2 = 0; g2 < 2; ++g2) {
-          const int g = 2 * gp + g2;
-          if (g >= P.ne) continue;
-          const size_t off = cb + slab * (g + (size_t)P.ne * iz2);
+          if (2 * gp + g2 >= P.ne) continue;
 #pragma unroll
           for (int o = lane * 2; o < VSZ / 2; o += 64) {
-            cp_async16(dst + C::ST_VI + g2 * (VSZ / 2) + o, P.vi + off + o);
-            if (!first) cp_async16(dst + C::ST_VO + g2 * (VSZ / 2) + o, P.vo + off + o);
+            cp_async16(dst + C::ST_VI + g2 * (VSZ / 2) + o, P.vi + off0 + g2 * slab + o);
+            if (!first) cp_async16(dst + C::ST_VO + g2 * (VSZ / 2) + o, P.vo + off0 + g2 * slab + o);
           }
         }
       }
       cp_async_commit();
     };
-    if (task != cur_task) {
-      prefetch(s, G);
-      prefetch(s + 1, G + 1);
-    }
-    prefetch(s + 2, G + 2);
-    cur_task = task;
-    cp_async_wait<2>();  // this step's group has landed (this thread's copies)
-    __syncwarp();        // ... and every lane's
-
-    const int c = s - wa - wb;
-    if (wa < w && wb < h && c >= 0 && c < nzr) {
-      const int ix = dx > 0 ? x0 + wa : x1 - 1 - wa;
-      const int iy = dy > 0 ? y0 + wb : y1 - 1 - wb;
-      const int iz = dz > 0 ? z0 + c : z1 - 1 - c;
-      const int g_col = 2 * gp + (q >> 2), u_col = q & 3;
-      const bool gval = g_col < P.ne;
-      const int g_vo = 2 * gp + (r >> 1);
-
-      // vi fragments from the stage (zero for a missing second group)
-      double vif[KS];
-      {
-        const double* src = stg + C::ST_VI + warp * VSZ + (q >> 2) * (VSZ / 2) + NM_ * u_col + KS * r;
+    auto load_vi = [&](const double* stage, double (&vf)[KS]) {
+      const double* src = stage + C::ST_VI + warp * VSZ + vi_lane;
 #pragma unroll
-        for (int k = 0; k < KS; ++k) vif[k] = gval ? src[k] : 0.0;
+      for (int k = 0; k < KS; ++k) vf[k] = gval ? src[k] : 0.0;
+    };
+    // moments -> angles of one t-tile (FP64 tensor-core products)
+    auto transform1 = [&](const double (&vf)[KS], int ch, int t, double (&d)[2]) {
+      d[0] = d[1] = 0.0;
+#pragma unroll
+      for (int k = 0; k < KS; ++k) {
+        const double b = NCH == 1 ? b1r[NCH == 1 ? k : 0][t] : mat[((ch * KS + k) * 4 + t) * 32 + lane];
+        dmma(d, vf[k], b);
       }
+    };
+    prefetch(0, G);
+    prefetch(1, G + 1);
+    prefetch(2, G + 2);
 
-      const double so = (double)(1 + oct);
-      const double so_r = 1.0 / so;
-      const double s_sp = (double)d_scale_space(ix, iy, iz);
-      const double cxy = 0.5 / (double)d_scale_space(ix, iy, iz - dz);
-      const double cxz = 0.25 / (double)d_scale_space(ix, iy - dy, iz);
-      const double sx_r = 1.0 / (double)d_scale_space(ix - dx, iy, iz);
-      const double cyz[2] = {wz[0] * sx_r, wz[1] * sx_r};
-      const double cc = so_r * s_sp;
-
-      const int prev = (int)((G - 1) & 1), cur = (int)(G & 1);
-      double* const slot_yz = slots;                  // [2][NW][ENT]
-      double* const slot_xz = slots + 2 * NW * ENT;   // [2][NW][ENT]
-      // where the three incoming faces come from
-      const double* in_yz = nullptr;  // smem (neighbour warp or stage) ...
-      const double* gin_yz = nullptr; // ... or global (NCH > 1 edge warps)
-      const double* in_xz = nullptr;
-      const double* gin_xz = nullptr;
-      const double* in_xy = nullptr;
-      const double* gin_xy = nullptr;
-      const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
-      const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;
-      if (wa > 0) in_yz = slot_yz + (size_t)(prev * NW + warp - 1) * ENT;
-      else if (flags & TF_X_IN) {
-        if constexpr (C::FACE_PF) in_yz = stg + C::ST_YZ + wb * ENT;
-        else gin_yz = P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT;
+    bool stop = false;
+    for (int s = 0; s < nsteps; ++s, ++G) {
+      const int st = (int)(G % NS);
+      const double* stg = stages + (size_t)st * C::STAGE;
+      if (s > 0) {
+        if (!mbar_wait(&full[st], (uint32_t)((G / NS) & 1), P.sy, -1)) { stop = true; break; }
+        if (reinterpret_cast<const StepHdr*>(stg + C::ST_HDR)->stop) { stop = true; break; }
       }
-      if (wb > 0) in_xz = slot_xz + (size_t)(prev * NW + warp - TX) * ENT;
-      else if (flags & TF_Y_IN) {
-        if constexpr (C::FACE_PF) in_xz = stg + C::ST_XZ + wa * ENT;
-        else gin_xz = P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT;
-      }
-      if (c == 0 && (flags & TF_Z_IN)) {
-        if constexpr (C::FACE_PF) in_xy = stg + C::ST_XY + wb * ENT;
-        else gin_xy = P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT;
-      }
-      double* out_yz = slot_yz + (size_t)(cur * NW + warp) * ENT;
-      double* out_xz = slot_xz + (size_t)(cur * NW + warp) * ENT;
-      double* gout_yz = (wa == w - 1 && (flags & TF_X_OUT)) ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT : nullptr;
-      double* gout_xz = (wb == h - 1 && (flags & TF_Y_OUT)) ? P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT : nullptr;
-      double* gout_xy = (c == nzr - 1 && (flags & TF_Z_OUT)) ? P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT : nullptr;
+      prefetch(s + 3, G + 3);
+      cp_async_wait<2>();  // the groups of steps s and s+1 have landed (this thread's copies)
+      __syncwarp();        // ... and every lane's
 
-      double d2[MT][2][2];  // two accumulators per m-tile (even / odd t)
+      const int c = s - cbeg;
+      if (act && c >= 0 && c < nzr) {
+        const int iz = iz0 + dz * c;
+        const int prev = (int)((G - 1) & 1), cur = (int)(G & 1);
+        // solve coefficients: powers of two except so_r
+        const double cxy = d_pow2(-1 - ((sp_xy + 7 * (iz - dz)) & 3));
+        const double cxz = d_pow2(-2 - ((sp_xy - 3 * dy + 7 * iz) & 3));
+        const double sx_r = d_pow2(-((sp_xy - dx + 7 * iz) & 3));
+        const double cyz[2] = {wz[0] * sx_r, wz[1] * sx_r};
+        const double cc = so_r * d_pow2((sp_xy + 7 * iz) & 3);
+
+        // where the three incoming faces come from
+        const double* in_yz = wa > 0 ? slot_yz + (size_t)(prev * NW + warp - 1) * ENT
+                              : (x_in && C::FACE_PF) ? stg + C::ST_YZ + wb * ENT : nullptr;
+        const double* gin_yz = (!C::FACE_PF && x_in) ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT : nullptr;
+        const double* in_xz = wb > 0 ? slot_xz + (size_t)(prev * NW + warp - TX) * ENT
+                              : (y_in && C::FACE_PF) ? stg + C::ST_XZ + wa * ENT : nullptr;
+        const double* gin_xz = (!C::FACE_PF && y_in) ? P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT : nullptr;
+        const double* in_xy = (c == 0 && z_in && C::FACE_PF) ? stg + C::ST_XY + wb * ENT : nullptr;
+        const double* gin_xy = (c == 0 && z_in && !C::FACE_PF) ? P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT : nullptr;
+        double* out_yz = slot_yz + (size_t)(cur * NW + warp) * ENT;
+        double* out_xz = slot_xz + (size_t)(cur * NW + warp) * ENT;
+        double* gout_yz = x_out ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT : nullptr;
+        double* gout_xz = y_out ? P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT : nullptr;
+        double* gout_xy = (c == nzr - 1 && z_out) ? P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT : nullptr;
+        const int gx = dx > 0 ? -1 : P.nx, gy = dy > 0 ? -1 : P.ny, gz = dz > 0 ? -1 : P.nz;  // ghost cells
+
+        const bool has_next = PIPE_T1 && c + 1 < nzr;
+        double vin[KS];
+        if (has_next) load_vi(stages + (size_t)((G + 1) % NS) * C::STAGE, vin);
+        if (!PIPE_T1 || c == 0) {
+          double vif[KS];
+          load_vi(stg, vif);
 #pragma unroll
-      for (int mt = 0; mt < MT; ++mt) d2[mt][0][0] = d2[mt][0][1] = d2[mt][1][0] = d2[mt][1][1] = 0.0;
+          for (int ch = 0; ch < NCH; ++ch)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) transform1(vif, ch, t, d1n[ch][t]);
+        }
+
+        double d2[MT][2][2];  // two accumulators per m-tile (even / odd t)
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) d2[mt][0][0] = d2[mt][0][1] = d2[mt][1][0] = d2[mt][1][1] = 0.0;
 
 #pragma unroll
-      for (int ch = 0; ch < NCH; ++ch) {
-        // ---- moments -> angles
-        double d1[4][2];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) d1[t][0] = d1[t][1] = 0.0;
-#pragma unroll
-        for (int k = 0; k < KS; ++k)
+        for (int ch = 0; ch < NCH; ++ch) {
 #pragma unroll
           for (int t = 0; t < 4; ++t) {
-            const double b = NCH == 1 ? b1r[NCH == 1 ? k : 0][t] : mat[((ch * KS + k) * 4 + t) * 32 + lane];
-            dmma(d1[t], vif[k], b);
-          }
-
+            double d1[2] = {d1n[ch][t][0], d1n[ch][t][1]};
+            // the next plane's moments -> angles does not depend on this
+            // plane's faces: interleave it with this plane's solve
+            if (has_next) transform1(vin, ch, t, d1n[ch][t]);
+            const int eo = ((ch * 4 + t) * 32 + lane) * 2;
+            double fyz[2], fxz[2], fxy[2];
+            if (in_yz) {
+              const double2 v = *reinterpret_cast<const double2*>(in_yz + eo);
+              fyz[0] = v.x; fyz[1] = v.y;
+            } else if (gin_yz) {
+              const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_yz + eo));
+              fyz[0] = v.x; fyz[1] = v.y;
+            } else {
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const size_t eo = (size_t)((ch * 4 + t) * 32 + lane) * 2;
-          double fyz[2], fxz[2], fxy[2];
-          if (in_yz) {
-            const double2 v = *reinterpret_cast<const double2*>(in_yz + eo);
-            fyz[0] = v.x; fyz[1] = v.y;
-          } else if (gin_yz) {
-            const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_yz + eo));
-            fyz[0] = v.x; fyz[1] = v.y;
-          } else {
+              for (int i = 0; i < 2; ++i) {
+                const int ia = 32 * ch + 8 * t + 2 * r + i;
+                fyz[i] = ia < P.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(gx, iy, iz)) * face_k : 0.0;
+              }
+            }
+            if (in_xz) {
+              const double2 v = *reinterpret_cast<const double2*>(in_xz + eo);
+              fxz[0] = v.x; fxz[1] = v.y;
+            } else if (gin_xz) {
+              const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_xz + eo));
+              fxz[0] = v.x; fxz[1] = v.y;
+            } else {
+#pragma unroll
+              for (int i = 0; i < 2; ++i) {
+                const int ia = 32 * ch + 8 * t + 2 * r + i;
+                fxz[i] = ia < P.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, gy, iz)) * face_k : 0.0;
+              }
+            }
+            if (c > 0) {
+              fxy[0] = carry[ch][t][0]; fxy[1] = carry[ch][t][1];
+            } else if (in_xy) {
+              const double2 v = *reinterpret_cast<const double2*>(in_xy + eo);
+              fxy[0] = v.x; fxy[1] = v.y;
+            } else if (gin_xy) {
+              const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_xy + eo));
+              fxy[0] = v.x; fxy[1] = v.y;
+            } else {
+#pragma unroll
+              for (int i = 0; i < 2; ++i) {
+                const int ia = 32 * ch + 8 * t + 2 * r + i;
+                fxy[i] = ia < P.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, iy, gz)) * face_k : 0.0;
+              }
+            }
+
+            // ---- Quantities_solve, exact 7-operation form (no contraction)
+            double out[2];
 #pragma unroll
             for (int i = 0; i < 2; ++i) {
-              const int ia = 32 * ch + 8 * t + 2 * r + i;
-              fyz[i] = (gval && ia < P.na) ? d_init_face(ia, dx > 0 ? -1 : P.nx, iy, iz, g_col, u_col, oct) : 0.0;
+              const double bxz = __dmul_rn(fxz[i], cxz);
+              const double sab = __fma_rn(fxy[i], cxy, bxz);  // fxy*cxy is exact
+              const double cyzv = __dmul_rn(fyz[i], cyz[i]);
+              const double sm = __dadd_rn(sab, cyzv);
+              const double psi = __dadd_rn(d1[i], __dmul_rn(sm, cc));
+              d1[i] = psi;
+              out[i] = __dmul_rn(psi, so);
+              carry[ch][t][i] = out[i];
             }
-          }
-          if (in_xz) {
-            const double2 v = *reinterpret_cast<const double2*>(in_xz + eo);
-            fxz[0] = v.x; fxz[1] = v.y;
-          } else if (gin_xz) {
-            const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_xz + eo));
-            fxz[0] = v.x; fxz[1] = v.y;
-          } else {
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-              const int ia = 32 * ch + 8 * t + 2 * r + i;
-              fxz[i] = (gval && ia < P.na) ? d_init_face(ia, ix, dy > 0 ? -1 : P.ny, iz, g_col, u_col, oct) : 0.0;
-            }
-          }
-          if (c > 0) {
-            fxy[0] = carry[ch][t][0]; fxy[1] = carry[ch][t][1];
-          } else if (in_xy) {
-            const double2 v = *reinterpret_cast<const double2*>(in_xy + eo);
-            fxy[0] = v.x; fxy[1] = v.y;
-          } else if (gin_xy) {
-            const double2 v = __ldcg(reinterpret_cast<const double2*>(gin_xy + eo));
-            fxy[0] = v.x; fxy[1] = v.y;
-          } else {
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-              const int ia = 32 * ch + 8 * t + 2 * r + i;
-              fxy[i] = (gval && ia < P.na) ? d_init_face(ia, ix, iy, dz > 0 ? -1 : P.nz, g_col, u_col, oct) : 0.0;
-            }
-          }
+            const double2 ov = make_double2(out[0], out[1]);
+            *reinterpret_cast<double2*>(out_yz + eo) = ov;
+            *reinterpret_cast<double2*>(out_xz + eo) = ov;
+            if (gout_yz) __stcg(reinterpret_cast<double2*>(gout_yz + eo), ov);
+            if (gout_xz) __stcg(reinterpret_cast<double2*>(gout_xz + eo), ov);
+            if (gout_xy) __stcg(reinterpret_cast<double2*>(gout_xy + eo), ov);
 
-          // ---- Quantities_solve, exact 7-operation form (no contraction)
-          double out[2];
+            // ---- angles -> moments for this t (psi is the B operand as is)
 #pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const double bxz = __dmul_rn(fxz[i], cxz);
-            const double sab = __fma_rn(fxy[i], cxy, bxz);  // fxy*cxy is exact
-            const double cyzv = __dmul_rn(fyz[i], cyz[i]);
-            const double sm = __dadd_rn(sab, cyzv);
-            const double psi = __dadd_rn(d1[t][i], __dmul_rn(sm, cc));
-            d1[t][i] = psi;
-            out[i] = __dmul_rn(psi, so);
-            carry[ch][t][i] = out[i];
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+              for (int mt = 0; mt < MT; ++mt) {
+                const double a = NCH == 1 ? a2r[NCH == 1 ? mt : 0][t][i]
+                                          : mat[NCH * KS * 4 * 32 + ((((ch * MT + mt) * 4 + t) * 2 + i) * 32) + lane];
+                dmma(d2[mt][t & 1], a, d1[i]);
+              }
           }
-          const double2 ov = make_double2(out[0], out[1]);
-          *reinterpret_cast<double2*>(out_yz + eo) = ov;
-          *reinterpret_cast<double2*>(out_xz + eo) = ov;
-          if (gout_yz) __stcg(reinterpret_cast<double2*>(gout_yz + eo), ov);
-          if (gout_xz) __stcg(reinterpret_cast<double2*>(gout_xz + eo), ov);
-          if (gout_xy) __stcg(reinterpret_cast<double2*>(gout_xy + eo), ov);
+        }
 
-          // ---- angles -> moments for this t (psi is the B operand as is)
+        // ---- accumulate vo in the region's visiting order
+        if (gvo) {
+          double* vdst = P.vo + col + slab * (size_t)g_vo + (size_t)(slab * P.ne) * (size_t)iz + (vo_lane - (r >> 1) * (VSZ / 2));
+          const double* vold = stg + C::ST_VO + warp * VSZ + vo_lane;
 #pragma unroll
-          for (int i = 0; i < 2; ++i)
+          for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-              const double a = NCH == 1 ? a2r[NCH == 1 ? mt : 0][t][i]
-                                        : mat[NCH * KS * 4 * 32 + ((((ch * MT + mt) * 4 + t) * 2 + i) * 32) + lane];
-              dmma(d2[mt][t & 1], a, d1[t][i]);
+            for (int j = 0; j < 2; ++j) {
+              if (8 * mt + q < NM_) {
+                const int o = NM_ * j + 8 * mt;
+                const double dsum = __dadd_rn(d2[mt][0][j], d2[mt][1][j]);
+                vdst[o] = first ? dsum : __dadd_rn(vold[o], dsum);
+              }
             }
         }
       }
-
-      // ---- accumulate vo in the region's visiting order
-      if (g_vo < P.ne) {
-        const size_t vbase = (size_t)NM_ * NU * (ix + (size_t)P.nx * iy) + slab * (g_vo + (size_t)P.ne * iz);
-        const double* vold = stg + C::ST_VO + warp * VSZ + (r >> 1) * (VSZ / 2);
-#pragma unroll
-        for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-          for (int j = 0; j < 2; ++j) {
-            const int im = 8 * mt + q;
-            if (im < NM_) {
-              const int o = NM_ * (2 * (r & 1) + j) + im;
-              const double dsum = __dadd_rn(d2[mt][0][j], d2[mt][1][j]);
-              P.vo[vbase + o] = first ? dsum : __dadd_rn(vold[o], dsum);
-            }
-          }
-      }
+      // step G done by this warp: its writes are ordered before the arrive;
+      // once every compute warp has arrived, the neighbours' faces of step G
+      // are visible and step G + 1 may start
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&done[st]);
+      if (!mbar_wait(&done[st], (uint32_t)((G / NS) & 1), P.sy, -1)) { stop = true; break; }
     }
-    // step G done by this warp: its writes are ordered before the arrive;
-    // once every compute warp has arrived, the neighbours' faces of step G
-    // are visible and step G + 1 may start
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&done[st]);
-    if (!mbar_wait(&done[st], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
+    if (stop) break;
   }
   cp_async_wait<0>();  // no copy into shared memory outlives the CTA
 }

@@ -27,13 +27,17 @@ struct Variant {
 };
 
 constexpr int kStages = 4;
+#ifndef MSB_PIPE_T1
+#define MSB_PIPE_T1 false
+#endif
+constexpr bool kPipeT1 = MSB_PIPE_T1;
 
 template <int NM_, int NCH, int TX, int TY>
 Variant make_variant() {
   using C = Fp64Cfg<NM_, NCH, TX, TY, kStages>;
   static_assert(C::smem_bytes() <= 227 * 1024, "shared memory budget");
   Variant v;
-  v.fn = sweep_fp64_kernel<NM_, NCH, TX, TY, kStages>;
+  v.fn = sweep_fp64_kernel<NM_, NCH, TX, TY, kStages, kPipeT1>;
   v.smem = C::smem_bytes();
   v.tx = TX;
   v.ty = TY;
