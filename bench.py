@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 KBA sweep (minisweep's Sweeper_sweep hot path).
+
+Workload: 64^3 cells, ne 64, na 32 angles per octant, NM 16 moments, NU 4,
+nblock_z 8, niterations 10, the built-in deterministic Quantities, FP64 plain.
+One step = one run of the reference driver's iteration loop (runner.c:148-155):
+10 sweeps with the vi/vo swap.  Metric: cell-angle-group updates per second,
+one update = one (cell, angle, group, octant) solve, 64^3 * 32 * 64 * 8 per
+sweep.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank sweeps its own 64-group slice (energy groups are
+independent: no data exchange); the per-GPU work is fixed, so scaling is weak.
+The reference arm times the reference's own OpenMP CPU sweep (built from its
+sources into oracle/_ref) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+NX = NY = NZ = 64
+NE, NA, NM, NU, NBLOCK_Z, NITER = 64, 32, 16, 4, 8, 10
+METRIC = "cell-angle-group updates/s, FP64 plain vs mixed-precision at stated error"
+UNIT = "updates/s"
+WORKLOAD = (f"minisweep KBA sweep, {NX}x{NY}x{NZ} cells, ne {NE}, na {NA}, NM {NM}, NU {NU}, "
+            f"nblock_z {NBLOCK_Z}, niterations {NITER}, built-in Quantities, FP64 plain")
+
+
+def updates_per_sweep(nx=NX, ny=NY, nz=NZ, ne=NE, na=NA) -> int:
+    return nx * ny * nz * ne * na * 8
+
+
+def flops_per_sweep(nx=NX, ny=NY, nz=NZ, ne=NE, na=NA, nm=NM) -> float:
+    # the reference's flop model (runner.c:162-166): two transforms + 12 per solve
+    state = nx * ny * nz * ne * nm * NU
+    return state * 8 * 2.0 * na * 2 + nx * ny * nz * ne * na * NU * 8 * 12.0
+
+
+def config_dict(ne=NE) -> dict:
+    return {"workload": WORKLOAD, "ncell": [NX, NY, NZ], "ne_per_gpu": ne, "na": NA, "nm": NM, "nu": NU,
+            "nblock_z": NBLOCK_Z, "niterations": NITER,
+            "l2": "state arrays of 8.6 GB each, far above the 126 MB L2: no flush needed between steps"}
+
+
+# ------------------------------------------------------------------ helpers
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out = self.proc.communicate()[0]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def profile_traffic() -> float | None:
+    """DRAM bytes per sweep of the FP64 kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "sweep_fp64_kernel.md")) as f:
+            m = re.search(r"traffic_bytes_per_sweep_64cubed:\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def reference_binary() -> str | None:
+    p = os.path.join(ROOT, "oracle", "_ref", f"sweep_omp_nm{NM}")
+    return p if os.access(p, os.X_OK) else None
+
+
+def cpu_sample(ne_sample: int | None = None):
+    """One bounded run of the reference OpenMP sweep on the host cores.
+    Returns (updates/s, seconds, threads, description) or None."""
+    binp = reference_binary()
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    nthr = max(1, min(NE, cores or 1))
+    ne = ne_sample or nthr
+    if binp is None:
+        return None
+    env = dict(os.environ, OMP_NUM_THREADS=str(nthr), OMP_PROC_BIND="true")
+    args = [binp, "--ncell_x", str(NX), "--ncell_y", str(NY), "--ncell_z", str(NZ), "--ne", str(ne),
+            "--na", str(NA), "--nblock_z", str(NBLOCK_Z), "--nthread_e", str(nthr), "--nthread_octant", "1",
+            "--niterations", "1"]
+    out = subprocess.run(args, env=env, capture_output=True, text=True, timeout=900).stdout
+    m = re.search(r"time:\s*([0-9.]+)", out)
+    ok = "PASS" in out
+    if not m or not ok:
+        return None
+    sec = float(m.group(1))
+    u = updates_per_sweep(ne=ne)
+    desc = (f"reference OpenMP sweep (oracle/_ref/sweep_omp_nm{NM}, --nthread_e {nthr}), "
+            f"{NX}^3 cells x ne {ne} x na {NA}, 1 sweep ({u:.3g} updates, {sec:.2f} s)")
+    return u / sec, sec, nthr, desc
+
+
+def cpu_sample_port():
+    """Fallback when the reference build is absent: the oracle port, 1 thread."""
+    import numpy as np
+
+    import oracle
+    nx = ny = nz = 16
+    ne = 8
+    a, m = oracle.am_matrices(NM, NA)
+    vi = oracle.init_state(nx, ny, nz, ne, NM)
+    t0 = time.perf_counter()
+    oracle.sweep(nx, ny, nz, ne, NM, NA, a, m, vi)
+    sec = time.perf_counter() - t0
+    u = updates_per_sweep(nx, ny, nz, ne, NA)
+    del np
+    return u / sec, sec, 1, f"oracle port (oracle/sweep_oracle.c), {nx}^3 x ne {ne} x na {NA}, 1 thread"
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args, rank: int) -> int:
+    if rank != 0:
+        return 0
+    vals, secs = [], []
+    kind = "reference"
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample()
+        if r is None:
+            kind = "port"
+            r = cpu_sample_port()
+        if i >= args.warmup:
+            vals.append(r[0])
+            secs.append(r[1])
+        nthr, desc = r[2], r[3]
+    v = sorted(vals)[len(vals) // 2]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: the reference's built-in deterministic Quantities", "config": config_dict(),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthr, "kind": kind, "sample": desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank: int, world: int, local_rank: int) -> int:
+    import torch
+
+    import minisweep_b200 as msb
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    flags = (f"--ncell_x {NX} --ncell_y {NY} --ncell_z {NZ} --ne {NE} --na {NA} --nblock_z {NBLOCK_Z} "
+             f"--niterations {NITER}")
+    pb = msb.Problem(flags, nm=NM)
+    n = pb.nstate
+    va = torch.empty(n, dtype=torch.float64, device=dev)
+    vb = torch.empty(n, dtype=torch.float64, device=dev)
+    pb.init_state_device(va.data_ptr())
+    stream = torch.cuda.ExternalStream(pb.stream)
+    torch.cuda.synchronize()
+    peak_dmma, peak_dfma = msb.fp64_peak(5)
+
+    def one_step(evs=None):
+        a, b = va, vb
+        for _ in range(NITER):
+            if evs is not None:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(stream)
+                evs.append(e)
+            pb.sweep_device(b.data_ptr(), a.data_ptr())
+            a, b = b, a
+        if evs is not None:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(stream)
+            evs.append(e)
+
+    for _ in range(args.warmup):
+        one_step()
+    pb.sync()
+    barrier()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    evs = []
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for _ in range(args.steps):
+        one_step(evs)
+    t_end.record(stream)
+    pb.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    sweep_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(len(evs) - 1) if (i + 1) % (NITER + 1) != 0]
+    if dist is not None:
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    barrier()
+
+    # correctness of the timed result (built-in Quantities: vo == vi exactly)
+    normsq, normsqdiff = pb.norms_device(va.data_ptr(), vb.data_ptr())
+    closed = None
+    try:
+        import oracle
+        closed = oracle.normsq_closed_form(NX, NY, NZ, NE, NM)
+    except Exception:  # the oracle is only the checker; the number stands without it
+        pass
+
+    # end to end through the C ABI: host vi in, 10 sweeps, host result out
+    host_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    host_out = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    pb.init_state_device(va.data_ptr())
+    torch.cuda.synchronize()
+    host_in.copy_(va)
+    del va, vb
+    torch.cuda.empty_cache()
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        pb.sweep_iterations_host(host_out.data_ptr(), host_in.data_ptr(), NITER)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = e0.elapsed_time(e1) / 1e3
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_ok = bool(torch.equal(host_out, host_in))
+
+    upd = updates_per_sweep() * NITER
+    value = upd * args.steps * world / elapsed
+    e2e_value = upd * e2e_steps * world / e2e_s
+    ms_sweep = sum(sweep_ms) / len(sweep_ms)
+    tf = flops_per_sweep() / (ms_sweep * 1e-3) / 1e12
+    hbm_bytes = 16.0 * NX * NY * NZ * NE * NM * NU  # read vi once, write vo once
+    peaks = measured_peaks()
+    traffic = profile_traffic()
+    roofline = {"bound": "tensor", "achieved": tf, "peak": peak_dmma, "unit": "TFLOP/s",
+                "frac": tf / peak_dmma if peak_dmma else None,
+                "traffic": traffic,
+                "peak_source": "FP64 mma.sync peak measured live by msb_measure_fp64_peak (MEASURED_PEAKS.json "
+                               "has no FP64 figure); FMA-pipe FP64 peak %.2f TF/s" % peak_dfma,
+                "algorithmic": "reference flop model (runner.c:162-166) %.4g flop per sweep / mean sweep "
+                               "kernel time %.2f ms" % (flops_per_sweep(), ms_sweep),
+                "hbm_view": {"achieved_gbs": hbm_bytes / (ms_sweep * 1e-3) / 1e9,
+                             "peak_gbs": peaks.get("hbm_gbs"),
+                             "note": "algorithmic bytes 16 x state (vi read + vo write); the FP64 path is "
+                                     "FP64-compute-bound, not HBM-bound"}}
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            r = cpu_sample(ne_sample=None)
+            kind = "reference"
+            if r is None:
+                r = cpu_sample_port()
+                kind = "port"
+            cpu = {"value": r[0], "unit": UNIT, "cores": r[2], "kind": kind, "sample": r[3]}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: the reference's built-in deterministic Quantities (index-derived state, "
+                        "faces and transform matrices)",
+                "config": dict(config_dict(), parallelism=f"{world} GPU(s) x 64-group slice, no exchange"),
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                        "d2h_bytes_per_step": 8 * n,
+                        "path": "Sweeper_sweep_iterations (host vi in, 10 device sweeps, host result out)",
+                        "result_matches": e2e_ok},
+                "clocks": clk, "gpu_launches": args.steps * NITER,
+                "check": {"normsq": normsq, "normsqdiff": normsqdiff, "normsq_closed_form": closed,
+                          "pass": normsqdiff == 0.0 and (closed is None or normsq == closed)},
+                "ms_per_sweep_kernel": ms_sweep}
+        print(json.dumps(line), flush=True)
+    pb.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -318,6 +318,12 @@ int Sweeper_sweep_status(Sweeper* sweeper, Pointer* vo, Pointer* vi,
 int Sweeper_sweep_device(Sweeper* sweeper, double* vo_d, const double* vi_d,
                          const Quantities* quan, Env* env);
 int Sweeper_sync_status(Sweeper* sweeper, Env* env);
+/* The reference driver's iteration loop (runner.c:148-155) in one call:
+ * v_in_h (host) is copied to the device once, niterations sweeps alternate
+ * between two device arrays, and the last sweep's output is copied to v_out_h
+ * (host).  Synchronous; returns the status of the device work. */
+int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const double* v_in_h, int niterations,
+                             const Quantities* quan, Env* env);
 /* Device-side FP64 checksums of two device state arrays (same sums as
  * get_state_norms). */
 int msb_state_norms_device(const double* vi_d, const double* vo_d, size_t n,

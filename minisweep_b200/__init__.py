@@ -89,6 +89,9 @@ def lib() -> ctypes.CDLL:
         L.Sweeper_sweep_status.argtypes = [P(Sweeper), P(Pointer), P(Pointer), P(Quantities), P(Env)]
         L.Sweeper_sweep_device.argtypes = [P(Sweeper), ctypes.c_void_p, ctypes.c_void_p, P(Quantities), P(Env)]
         L.Sweeper_sync_status.argtypes = [P(Sweeper), P(Env)]
+        L.Sweeper_sweep_iterations.argtypes = [P(Sweeper), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               P(Quantities), P(Env)]
+        L.msb_measure_fp64_peak.argtypes = [P(D), P(D), ctypes.c_int]
         L.Sweeper_last_stats.argtypes = [P(Sweeper), P(ctypes.c_longlong), P(ctypes.c_int)]
         L.Sweeper_debug_tasks.argtypes = [P(Sweeper), P(ctypes.c_int), ctypes.c_longlong]
         L.Sweeper_debug_tasks.restype = ctypes.c_longlong
@@ -127,6 +130,13 @@ def schedule(nx, ny, nz, ne, tx=4, ty=2, gp_block=1) -> np.ndarray:
     out = np.zeros((n, TASK_INTS), dtype=np.int32)
     L.msb_schedule_tasks(nx, ny, nz, ne, tx, ty, gp_block, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
     return out
+
+
+def fp64_peak(reps: int = 5):
+    """Measured FP64 throughput of this GPU (TFLOP/s): (tensor-core mma, FMA pipe)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(lib().msb_measure_fp64_peak(ctypes.byref(a), ctypes.byref(b), reps))
+    return a.value, b.value
 
 
 class Problem:
@@ -195,6 +205,12 @@ class Problem:
         """Enqueue vo = sweep(vi) on device arrays (async on self.stream)."""
         _check(lib().Sweeper_sweep_device(ctypes.byref(self.sweeper), ctypes.c_void_p(vo_ptr),
                                           ctypes.c_void_p(vi_ptr), ctypes.byref(self.quan), ctypes.byref(self.env)))
+
+    def sweep_iterations_host(self, out_ptr: int, in_ptr: int, niterations: int) -> None:
+        """Host buffers in and out, niterations device-resident sweeps (one C call)."""
+        _check(lib().Sweeper_sweep_iterations(ctypes.byref(self.sweeper), ctypes.c_void_p(out_ptr),
+                                              ctypes.c_void_p(in_ptr), niterations, ctypes.byref(self.quan),
+                                              ctypes.byref(self.env)))
 
     def sync(self) -> None:
         _check(lib().Sweeper_sync_status(ctypes.byref(self.sweeper), ctypes.byref(self.env)))

@@ -368,3 +368,32 @@ extern "C" int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit) {
   S->timeout_ns = limit > 0 ? limit : msb::kDefaultTimeoutNs;
   return MSB_OK;
 }
+
+// A whole run of the reference driver's iteration loop (runner.c:148-155) on
+// the device: v_in_h (host) is copied in once, niterations sweeps ping-pong
+// between two device arrays (the vi/vo swap), and the last sweep's output is
+// copied to v_out_h.  Pinned host buffers make the copies asynchronous.
+extern "C" int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const double* v_in_h, int niterations,
+                                        const Quantities* quan, Env* env) {
+  SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  if (!v_out_h || !v_in_h || niterations < 0) return msb::set_error(MSB_ERR_ARG, "invalid argument");
+  const size_t n = Dimensions_size_state(S->dims, NU);
+  cudaStream_t st = stream_of(env);
+  int rc;
+  if (!S->d_vi && (rc = msb::cuda_check(cudaMalloc(&S->d_vi, n * sizeof(double)), "cudaMalloc vi"))) return rc;
+  if (!S->d_vo && (rc = msb::cuda_check(cudaMalloc(&S->d_vo, n * sizeof(double)), "cudaMalloc vo"))) return rc;
+  if ((rc = msb::cuda_check(cudaMemcpyAsync(S->d_vi, v_in_h, n * sizeof(double), cudaMemcpyHostToDevice, st), "H2D")))
+    return rc;
+  double* a = S->d_vi;
+  double* b = S->d_vo;
+  for (int it = 0; it < niterations; ++it) {
+    if ((rc = Sweeper_sweep_device(sweeper, b, a, quan, env))) return rc;
+    double* tmp = a;
+    a = b;
+    b = tmp;
+  }
+  if ((rc = msb::cuda_check(cudaMemcpyAsync(v_out_h, a, n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H")))
+    return rc;
+  return msb::impl_sync(*S, st);
+}
