@@ -265,7 +265,55 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     except Exception:  # the oracle is only the checker; the number stands without it
         pass
 
+    def finish(e2e):
+        upd = updates_per_sweep() * NITER
+        value = upd * args.steps * world / elapsed
+        ms_sweep = sum(sweep_ms) / len(sweep_ms)
+        tf = flops_per_sweep() / (ms_sweep * 1e-3) / 1e12
+        hbm_bytes = 16.0 * NX * NY * NZ * NE * NM * NU  # read vi once, write vo once
+        peaks = measured_peaks()
+        traffic = profile_traffic()
+        roofline = {"bound": "tensor", "achieved": tf, "peak": peak_dmma, "unit": "TFLOP/s",
+                    "frac": tf / peak_dmma if peak_dmma else None,
+                    "traffic": traffic,
+                    "peak_source": "FP64 mma.sync peak measured live by msb_measure_fp64_peak (MEASURED_PEAKS.json "
+                                   "has no FP64 figure); FMA-pipe FP64 peak %.2f TF/s" % peak_dfma,
+                    "algorithmic": "reference flop model (runner.c:162-166) %.4g flop per sweep / mean sweep "
+                                   "kernel time %.2f ms" % (flops_per_sweep(), ms_sweep),
+                    "hbm_view": {"achieved_gbs": hbm_bytes / (ms_sweep * 1e-3) / 1e9,
+                                 "peak_gbs": peaks.get("hbm_gbs"),
+                                 "note": "algorithmic bytes 16 x state (vi read + vo write); the FP64 path is "
+                                         "FP64-compute-bound, not HBM-bound"}}
+        if rank == 0:
+            cpu = None
+            if world == 1 and not args.no_cpu:
+                r = cpu_sample(ne_sample=None)
+                kind = "reference"
+                if r is None:
+                    r = cpu_sample_port()
+                    kind = "port"
+                cpu = {"value": r[0], "unit": UNIT, "cores": r[2], "kind": kind, "sample": r[3]}
+            line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                    "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic: the reference's built-in deterministic Quantities (index-derived state, "
+                            "faces and transform matrices)",
+                    "config": dict(config_dict(), parallelism=f"{world} GPU(s) x 64-group slice, no exchange"),
+                    "roofline": roofline, "cpu_baseline": cpu,
+                    "e2e": e2e,
+                    "clocks": clk, "gpu_launches": args.steps * NITER,
+                    "check": {"normsq": normsq, "normsqdiff": normsqdiff, "normsq_closed_form": closed,
+                              "pass": normsqdiff == 0.0 and (closed is None or normsq == closed)},
+                    "ms_per_sweep_kernel": ms_sweep}
+            print(json.dumps(line), flush=True)
+        pb.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
     # end to end through the C ABI: host vi in, 10 sweeps, host result out
+    if args.no_e2e:
+        return finish(None)
     host_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
     host_out = torch.empty(n, dtype=torch.float64, pin_memory=True)
     pb.init_state_device(va.data_ptr())
@@ -288,55 +336,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_ok = bool(torch.equal(host_out, host_in))
-
-    upd = updates_per_sweep() * NITER
-    value = upd * args.steps * world / elapsed
-    e2e_value = upd * e2e_steps * world / e2e_s
-    ms_sweep = sum(sweep_ms) / len(sweep_ms)
-    tf = flops_per_sweep() / (ms_sweep * 1e-3) / 1e12
-    hbm_bytes = 16.0 * NX * NY * NZ * NE * NM * NU  # read vi once, write vo once
-    peaks = measured_peaks()
-    traffic = profile_traffic()
-    roofline = {"bound": "tensor", "achieved": tf, "peak": peak_dmma, "unit": "TFLOP/s",
-                "frac": tf / peak_dmma if peak_dmma else None,
-                "traffic": traffic,
-                "peak_source": "FP64 mma.sync peak measured live by msb_measure_fp64_peak (MEASURED_PEAKS.json "
-                               "has no FP64 figure); FMA-pipe FP64 peak %.2f TF/s" % peak_dfma,
-                "algorithmic": "reference flop model (runner.c:162-166) %.4g flop per sweep / mean sweep "
-                               "kernel time %.2f ms" % (flops_per_sweep(), ms_sweep),
-                "hbm_view": {"achieved_gbs": hbm_bytes / (ms_sweep * 1e-3) / 1e9,
-                             "peak_gbs": peaks.get("hbm_gbs"),
-                             "note": "algorithmic bytes 16 x state (vi read + vo write); the FP64 path is "
-                                     "FP64-compute-bound, not HBM-bound"}}
-    if rank == 0:
-        cpu = None
-        if world == 1 and not args.no_cpu:
-            r = cpu_sample(ne_sample=None)
-            kind = "reference"
-            if r is None:
-                r = cpu_sample_port()
-                kind = "port"
-            cpu = {"value": r[0], "unit": UNIT, "cores": r[2], "kind": kind, "sample": r[3]}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic: the reference's built-in deterministic Quantities (index-derived state, "
-                        "faces and transform matrices)",
-                "config": dict(config_dict(), parallelism=f"{world} GPU(s) x 64-group slice, no exchange"),
-                "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
-                        "d2h_bytes_per_step": 8 * n,
-                        "path": "Sweeper_sweep_iterations (host vi in, 10 device sweeps, host result out)",
-                        "result_matches": e2e_ok},
-                "clocks": clk, "gpu_launches": args.steps * NITER,
-                "check": {"normsq": normsq, "normsqdiff": normsqdiff, "normsq_closed_form": closed,
-                          "pass": normsqdiff == 0.0 and (closed is None or normsq == closed)},
-                "ms_per_sweep_kernel": ms_sweep}
-        print(json.dumps(line), flush=True)
-    pb.close()
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+    return finish({"value": updates_per_sweep() * NITER * e2e_steps * world / e2e_s, "unit": UNIT,
+                   "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                   "path": "Sweeper_sweep_iterations (host vi in, 10 device sweeps, host result out)",
+                   "result_matches": e2e_ok})
 
 
 def main() -> int:
@@ -346,7 +349,19 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--case", choices=["config2", "small"], default="config2",
+                    help="small: 32^3 cells, ne 32, one sweep per step, no e2e / CPU legs (profiling runs)")
     args = ap.parse_args()
+    if args.case == "small":
+        global NX, NY, NZ, NE, NITER, WORKLOAD
+        NX = NY = NZ = 32
+        NE, NITER = 32, 1
+        args.no_cpu = True
+        args.no_e2e = True
+        WORKLOAD = WORKLOAD.replace("64x64x64", "32x32x32").replace("ne 64", "ne 32").replace(
+            "niterations 10", "niterations 1")
+    else:
+        args.no_e2e = False
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

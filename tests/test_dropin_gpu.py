@@ -1,0 +1,62 @@
+"""The reference's own driver programs, unmodified, on the B200 library.
+
+oracle/Makefile's `dropin` target compiles the reference's src/4_driver/
+runner.c + sweep.c and runner.c + tester.c against include/ and links them
+with libminisweep_b200.so in place of the reference's libsweeper.  Here they
+run on the GPU: `sweep` must print the reference's result line with PASS and
+the reference's normsq, and `tester` must pass its whole battery (the
+compare_runs pairs of tester.c, each requiring normsqdiff == 0 and equal
+normsq across two flag sets).
+"""
+import os
+import re
+import subprocess
+
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+
+def binary(name):
+    p = os.path.join(REF, name)
+    if not os.access(p, os.X_OK):
+        pytest.skip(f"{name} not built (make -C oracle dropin)")
+    return p
+
+
+@pytest.mark.parametrize("nm,flags", [
+    (16, "--ncell_x 5 --ncell_y 4 --ncell_z 6 --ne 3 --na 32 --nblock_z 2"),
+    (16, "--ncell_x 8 --ncell_y 8 --ncell_z 8 --ne 8 --na 32 --niterations 3"),
+    (4, "--ncell_x 16 --ncell_y 16 --ncell_z 16 --ne 16 --na 32"),
+    (16, "--ncell_x 3 --ncell_y 5 --ncell_z 4 --ne 5 --na 33 --is_using_device 1 --nthread_octant 8 --nthread_e 5"),
+])
+def test_reference_sweep_driver(nm, flags):
+    out = subprocess.run([binary(f"sweep_b200_nm{nm}")] + flags.split(), capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    m = re.search(r"Normsq result: ([0-9.e+]+)\s+diff: ([0-9.e+-]+)\s+(PASS|FAIL)", out.stdout)
+    assert m, out.stdout
+    assert m.group(3) == "PASS" and float(m.group(2)) == 0.0
+    d = dict(zip(flags.split()[::2], flags.split()[1::2]))
+    ref = oracle.normsq_closed_form(int(d["--ncell_x"]), int(d["--ncell_y"]), int(d["--ncell_z"]),
+                                    int(d["--ne"]), nm)
+    assert abs(float(m.group(1)) - ref) <= 5e-9 * ref
+
+
+def test_reference_sweep_driver_rejects_bad_flags():
+    # Insist -> message + exit(EXIT_FAILURE), as the reference does
+    out = subprocess.run([binary("sweep_b200_nm16"), "--ncell_z", "5", "--nblock_z", "2"], capture_output=True,
+                         text=True, timeout=120)
+    assert out.returncode != 0
+    assert "Insist" in out.stderr
+
+
+def test_reference_tester_battery():
+    out = subprocess.run([binary("tester_b200_nm16")], capture_output=True, text=True, timeout=1200)
+    assert out.returncode == 0, out.stderr[-2000:]
+    m = re.search(r"TESTS\s+(\d+)\s+PASSED\s+(\d+)\s+FAILED\s+(\d+)", out.stdout)
+    assert m, out.stdout[-2000:]
+    assert int(m.group(1)) > 0 and m.group(1) == m.group(2) and int(m.group(3)) == 0
