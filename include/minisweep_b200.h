@@ -348,6 +348,25 @@ long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int
  * denominator of the FP64 sweep. */
 int msb_measure_fp64_peak(double* tflops_dmma, double* tflops_dfma, int reps);
 
+/* One FP64 sweep that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot allocate device memory when they sweep (their
+ * device memory is owned by a pool or arena, or they must not trigger the
+ * device synchronisation cudaMalloc/cudaFree can cause): every scratch buffer
+ * of the sweep (task table, progress counters, face planes) lives in one
+ * file-scope device array of MSB_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library holds until exit, and the schedule is built in static host
+ * arrays.  vo_d = sweep(vi_d) with the caller's device arrays (reference state
+ * and matrix layouts) on `stream`; returns after the sweep finished.
+ * Limits: NM 4 or 16, na <= 32, and the problem's scratch must fit the array
+ * (about 10^3 cells x 8 groups); larger problems return MSB_ERR_ARG with the
+ * bytes needed.  The first call on each device sets up (takes the array's
+ * device address with that device current): make it before any stream
+ * capture.  All calls share the array, which keeps the last call's contents;
+ * calls that overlap, on the GPU or on the host, race. */
+#define MSB_NOALLOC_SCRATCH_BYTES (32u << 20)
+int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double* a_from_m_d, const double* m_from_a_d,
+                      int ncell_x, int ncell_y, int ncell_z, int ne, int nm, int na, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
