@@ -192,6 +192,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     import torch
 
     import minisweep_b200 as msb
+    from minisweep_b200.parallel import max_over_ranks
 
     dist = None
     if world > 1:
@@ -250,10 +251,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     clk = clocks.stop()
     elapsed = t_start.elapsed_time(t_end) / 1e3
     sweep_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(len(evs) - 1) if (i + 1) % (NITER + 1) != 0]
-    if dist is not None:
-        t = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed)
     barrier()
 
     # correctness of the timed result (built-in Quantities: vo == vi exactly)
@@ -331,10 +329,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_s = e0.elapsed_time(e1) / 1e3
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s)
     e2e_ok = bool(torch.equal(host_out, host_in))
     return finish({"value": updates_per_sweep() * NITER * e2e_steps * world / e2e_s, "unit": UNIT,
                    "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
