@@ -44,7 +44,7 @@
 // two, so each rounded result equals the reference's 12-operation expression.
 #pragma once
 
-#include "sweep_common.cuh"
+#include "sweep_async.cuh"
 
 namespace msb {
 
@@ -68,85 +68,6 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// ---------------------------------------------------------------- mbarrier
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-  asm volatile(
-      "{\n .reg .b64 st;\n mbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(b))
-      : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile(
-      "{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 st, [%0], %1;\n}" ::"r"(
-          smem_u32(b)),
-      "r"(bytes)
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// 16-byte asynchronous copy global -> shared (L2 only) and its groups.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-// 1-D bulk copy global -> shared, completion counted on an mbarrier.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-
-// try_wait with a suspend-time hint: the warp sleeps in hardware until the
-// phase completes or about `ns` nanoseconds pass (no busy polling).
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity, uint32_t ns) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity), "r"(ns)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait on an mbarrier phase by a whole warp.  It does not give up
-// when another CTA aborts: inside a CTA every phase that was started is
-// completed (the loader finishes the stages it issued and then posts a stop),
-// so only a time-out ends it early.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const SyncArgs& s, int task) {
-  if (mbar_try_wait(b, parity, 20000)) return true;
-  const long long t0 = global_ns();
-  for (;;) {
-    if (mbar_try_wait(b, parity, 100000)) return true;
-    if (global_ns() - t0 > s.timeout_ns) {
-      if ((threadIdx.x & 31) == 0) raise_error(s.sync, MSB_ERR_TIMEOUT, task);
-      return false;
-    }
-  }
-}
-
-// Per-step header written by the producer into each stage.
-struct StepHdr {
-  int task, s, oct, gp;
-  int x0, x1, y0, y1, z0, z1;
-  int flags, mat;  // mat: which matrix buffer holds this task's octant
-  int stop, pad0, pad1, pad2;
-};
 
 template <int NM_, int NCH, int TX, int TY, int NS>
 struct Fp64Cfg {

@@ -4,26 +4,36 @@
 // flags as the reference, then builds the task schedule and the device
 // buffers (face planes per octant, schedule, progress counters).
 // Sweeper_sweep (sweeper_kba_c.h:588-845) is one persistent kernel launch.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
 #include <memory>
 #include <new>
+#include <type_traits>
 
 #include "internal.h"
 #include "sweep_fp64_ws.cuh"
+#include "sweep_mixed_tc.cuh"
 
 namespace msb {
 
 namespace {
 
 using KernelFn = void (*)(const Fp64Params);
+using MixKernelFn = void (*)(const MixParams);
 
+// One compiled kernel: the FP64 kernel (fn) or a mixed-precision one (mix).
 struct Variant {
   KernelFn fn = nullptr;
+  MixKernelFn mix = nullptr;
   size_t smem = 0;
+  size_t entry_bytes = 0;  // one face entry (octant, group pair, position)
   int tx = 0, ty = 0, nch = 0, threads = 0;
+  bool valid() const { return fn || mix; }
+  const void* func() const { return fn ? (const void*)fn : (const void*)mix; }
 };
 
 constexpr int kStages = 4;
@@ -39,6 +49,7 @@ Variant make_variant() {
   Variant v;
   v.fn = sweep_fp64_kernel<NM_, NCH, TX, TY, kStages, kPipeT1>;
   v.smem = C::smem_bytes();
+  v.entry_bytes = (size_t)NCH * 256 * sizeof(double);
   v.tx = TX;
   v.ty = TY;
   v.nch = NCH;
@@ -57,7 +68,41 @@ Variant pick_nch(int nch) {
   }
 }
 
-Variant pick_variant(int nm, int na) {
+constexpr int kMixStages = 4;
+
+template <int NM_, int FMT>
+Variant make_mixed() {
+  using C = MixCfg<NM_, kMixStages>;
+  static_assert(C::smem_bytes() + 128 <= 227 * 1024, "shared memory budget (dynamic + static)");
+  Variant v;
+  v.mix = sweep_mixed_kernel<NM_, FMT, kMixStages>;
+  v.smem = C::smem_bytes();
+  v.entry_bytes = C::EB;
+  v.tx = C::TX;
+  v.ty = C::TY;
+  v.nch = 1;
+  v.threads = C::NT;
+  return v;
+}
+
+template <int FMT>
+Variant pick_mixed(int nm) {
+  switch (nm) {
+    case 4: return make_mixed<4, FMT>();
+    case 8: return make_mixed<8, FMT>();
+    case 16: return make_mixed<16, FMT>();
+    default: return Variant();
+  }
+}
+
+// precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves
+// (the mixed kernels take na <= 32).
+Variant pick_variant(int nm, int na, int precision) {
+  if (precision == 1 || precision == 2) {
+    if (na > 32) return Variant();
+    return precision == 1 ? pick_mixed<MIX_F16>(nm) : pick_mixed<MIX_BF16>(nm);
+  }
+  if (precision != 0) return Variant();
   const int nch = (na + 31) / 32;
   switch (nm) {
     case 4: return pick_nch<4>(nch);
@@ -69,10 +114,54 @@ Variant pick_variant(int nm, int na) {
 
 constexpr long long kDefaultTimeoutNs = 4000000000LL;  // 4 s per wait
 
+// cuTensorMapEncodeTiled from the driver, through the runtime (no -lcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// The state array (im fastest, then iu, ix, iy, ie, iz) as a 5-D tensor
+// (moment, unknown * x, y, group, z) whose box is one cell: NM moments x 4
+// unknowns x 1 x (2 groups, 1 when ne == 1) x 1, copied with the swizzle the
+// mixed kernel reads with.
+int encode_state_map(CUtensorMap* map, const double* ptr, const Dimensions& d, int* box_bytes) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return set_error(MSB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  if (reinterpret_cast<uintptr_t>(ptr) % 16 != 0)
+    return set_error(MSB_ERR_ARG, "the mixed-precision sweep needs 16-byte aligned state arrays");
+  const cuuint64_t row = (cuuint64_t)d.nm * sizeof(double);
+  const cuuint64_t dims[5] = {(cuuint64_t)d.nm, (cuuint64_t)NU * d.ncell_x, (cuuint64_t)d.ncell_y, (cuuint64_t)d.ne,
+                              (cuuint64_t)d.ncell_z};
+  const cuuint64_t strides[4] = {row, row * NU * d.ncell_x, row * NU * d.ncell_x * d.ncell_y,
+                                 row * NU * d.ncell_x * d.ncell_y * d.ne};
+  const cuuint32_t ng = d.ne >= 2 ? 2 : 1;
+  const cuuint32_t box[5] = {(cuuint32_t)d.nm, (cuuint32_t)NU, 1, ng, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  const CUtensorMapSwizzle swz = d.nm == 16 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                 : d.nm == 8 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                             : CU_TENSOR_MAP_SWIZZLE_32B;
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double*>(ptr), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(MSB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  *box_bytes = (int)(d.nm * sizeof(double) * NU * ng);
+  return MSB_OK;
+}
+
 }  // namespace
 
 struct SweeperImpl {
   Dimensions dims{};
+  int precision = 0;
   int ngp = 0;
   int gp_block = 1;
   Variant var;
@@ -81,8 +170,8 @@ struct SweeperImpl {
   int* d_tasks = nullptr;
   int* d_sync = nullptr;
   size_t sync_ints = 0;
-  double* d_face[3] = {nullptr, nullptr, nullptr};  // xy, xz, yz
-  size_t face_doubles[3] = {0, 0, 0};
+  void* d_face[3] = {nullptr, nullptr, nullptr};  // xy, xz, yz
+  size_t face_bytes[3] = {0, 0, 0};
   double* d_afm = nullptr;
   double* d_mfa = nullptr;
   double* d_vi = nullptr;  // staging for host-only Pointers
@@ -103,14 +192,17 @@ struct SweeperImpl {
   }
 };
 
-static int impl_create(SweeperImpl& S, const Dimensions& dims) {
+static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision) {
   S.dims = dims;
+  S.precision = precision;
   if (dims.ncell_x <= 0 || dims.ncell_y <= 0 || dims.ncell_z <= 0 || dims.ne <= 0 || dims.na <= 0)
     return set_error(MSB_ERR_ARG, "invalid dimensions");
-  S.var = pick_variant(dims.nm, dims.na);
-  if (!S.var.fn)
-    return set_error(MSB_ERR_UNSUPPORTED, "no kernel variant for nm=%d na=%d (nm in {4,8,16}, na <= 128)",
-                     dims.nm, dims.na);
+  S.var = pick_variant(dims.nm, dims.na, precision);
+  if (!S.var.valid())
+    return set_error(MSB_ERR_UNSUPPORTED,
+                     "no kernel variant for nm=%d na=%d precision=%d (nm in {4,8,16}; na <= 128 for FP64, "
+                     "na <= 32 for the mixed kernels)",
+                     dims.nm, dims.na, precision);
   S.ngp = (dims.ne + 1) / 2;
   int rc, dev = 0, nsm = 0, occ = 0;
   if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
@@ -129,22 +221,21 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims) {
   if ((rc = cuda_check(cudaMalloc(&S.d_sync, S.sync_ints * sizeof(int)), "cudaMalloc sync"))) return rc;
   if ((rc = cuda_check(cudaMallocHost(&S.h_status, 8 * sizeof(int)), "cudaMallocHost status"))) return rc;
 
-  const size_t ent = (size_t)S.var.nch * 256;
-  const size_t per = (size_t)NOCTANT * S.ngp * ent;
-  S.face_doubles[0] = per * dims.ncell_y * dims.ncell_x;
-  S.face_doubles[1] = per * dims.ncell_z * dims.ncell_x;
-  S.face_doubles[2] = per * dims.ncell_z * dims.ncell_y;
+  const size_t per = (size_t)NOCTANT * S.ngp * S.var.entry_bytes;
+  S.face_bytes[0] = per * dims.ncell_y * dims.ncell_x;
+  S.face_bytes[1] = per * dims.ncell_z * dims.ncell_x;
+  S.face_bytes[2] = per * dims.ncell_z * dims.ncell_y;
   for (int f = 0; f < 3; ++f)
-    if ((rc = cuda_check(cudaMalloc(&S.d_face[f], S.face_doubles[f] * sizeof(double)), "cudaMalloc faces")))
-      return rc;
+    if ((rc = cuda_check(cudaMalloc(&S.d_face[f], S.face_bytes[f]), "cudaMalloc faces"))) return rc;
   const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
   if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
   if ((rc = cuda_check(cudaMalloc(&S.d_mfa, nmat * sizeof(double)), "cudaMalloc m_from_a"))) return rc;
 
-  if ((rc = cuda_check(cudaFuncSetAttribute(S.var.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S.var.smem),
+  if ((rc = cuda_check(cudaFuncSetAttribute(S.var.func(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)S.var.smem),
                        "cudaFuncSetAttribute")))
     return rc;
-  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, S.var.fn, S.var.threads,
+  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, S.var.func(), S.var.threads,
                                                                      S.var.smem),
                        "occupancy")))
     return rc;
@@ -174,25 +265,37 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
       return rc;
   }
   if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
-  Fp64Params P;
-  P.vi = vi_d;
-  P.vo = vo_d;
-  P.afm = S.d_afm;
-  P.mfa = S.d_mfa;
-  P.fxy = S.d_face[0];
-  P.fxz = S.d_face[1];
-  P.fyz = S.d_face[2];
-  P.tasks = S.d_tasks;
-  P.ntask = S.sched.ntask();
-  P.nx = S.dims.ncell_x;
-  P.ny = S.dims.ncell_y;
-  P.nz = S.dims.ncell_z;
-  P.ne = S.dims.ne;
-  P.na = S.dims.na;
-  P.ngp = S.ngp;
-  P.sy.sync = S.d_sync;
-  P.sy.timeout_ns = S.timeout_ns;
-  S.var.fn<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
+  auto fill = [&](auto& P, auto* face) {
+    using F = std::remove_pointer_t<decltype(face)>;
+    P.vi = vi_d;
+    P.vo = vo_d;
+    P.afm = S.d_afm;
+    P.mfa = S.d_mfa;
+    P.fxy = static_cast<F*>(S.d_face[0]);
+    P.fxz = static_cast<F*>(S.d_face[1]);
+    P.fyz = static_cast<F*>(S.d_face[2]);
+    P.tasks = S.d_tasks;
+    P.ntask = S.sched.ntask();
+    P.nx = S.dims.ncell_x;
+    P.ny = S.dims.ncell_y;
+    P.nz = S.dims.ncell_z;
+    P.ne = S.dims.ne;
+    P.na = S.dims.na;
+    P.ngp = S.ngp;
+    P.sy.sync = S.d_sync;
+    P.sy.timeout_ns = S.timeout_ns;
+  };
+  if (S.var.fn) {
+    Fp64Params P;
+    fill(P, (double*)nullptr);
+    S.var.fn<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
+  } else {
+    MixParams P;
+    fill(P, (float*)nullptr);
+    if ((rc = encode_state_map(&P.tm_vi, vi_d, S.dims, &P.vbox_bytes))) return rc;
+    if ((rc = encode_state_map(&P.tm_vo, vo_d, S.dims, &P.vbox_bytes))) return rc;
+    S.var.mix<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
+  }
   if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
                        "status copy")))
@@ -276,12 +379,13 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   sweeper->nthread_z = Arguments_consume_int_or_default(args, "--nthread_z", 1);
   if (sweeper->nthread_z <= 0) return bad("Invalid thread count supplied.");
   sweeper->precision = Arguments_consume_int_or_default(args, "--precision", 0);
-  if (sweeper->precision != 0) return msb::set_error(MSB_ERR_UNSUPPORTED, "--precision %d is not available", sweeper->precision);
+  if (sweeper->precision < 0 || sweeper->precision > 2)
+    return msb::set_error(MSB_ERR_ARG, "--precision must be 0 (FP64), 1 (mixed, FP16 halves) or 2 (mixed, BF16 halves)");
   (void)env;
 
   std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
   if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
-  const int rc = msb::impl_create(*S, dims);
+  const int rc = msb::impl_create(*S, dims, sweeper->precision);
   if (rc) return rc;
   sweeper->impl_ = S.release();
   return MSB_OK;

@@ -136,3 +136,23 @@ def test_unsupported_sizes_are_reported():
     assert rc in (msb.MSB_ERR_UNSUPPORTED, msb.MSB_ERR_CUDA)
     L.Quantities_destroy(ctypes.byref(q))
     L.Arguments_destroy(ctypes.byref(a))
+
+
+@pytest.mark.parametrize("flags,d,code", [
+    ("--precision 3", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),          # no such precision
+    ("--precision -1", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),
+    ("--precision 1", (4, 4, 4, 2, 16, 64), msb.MSB_ERR_UNSUPPORTED),  # mixed kernels take na <= 32
+    ("--precision 2", (4, 4, 4, 2, 12, 32), msb.MSB_ERR_UNSUPPORTED),  # NM 12
+])
+def test_precision_flag_checks(flags, d, code):
+    L = msb.lib()
+    env = msb.Env()
+    a = _args(flags)
+    q = msb.Quantities()
+    dims = msb.Dimensions(*d)
+    L.Quantities_create(ctypes.byref(q), dims, ctypes.byref(env))
+    sw = msb.Sweeper()
+    rc = L.Sweeper_create_status(ctypes.byref(sw), dims, ctypes.byref(q), ctypes.byref(env), ctypes.byref(a))
+    assert rc == code, msb.last_error()
+    L.Quantities_destroy(ctypes.byref(q))
+    L.Arguments_destroy(ctypes.byref(a))
