@@ -139,6 +139,21 @@ def fp64_peak(reps: int = 5):
     return a.value, b.value
 
 
+def random_matrices(nm: int, na: int, seed: int = 1234):
+    """Transform matrices of the random-input precision study, in the
+    reference layouts: a_from_m[oct][im][ia] drawn N(0, 1/nm) (numpy PCG64),
+    m_from_a[oct][ia][im] = its least-squares pseudo-inverse in FP64 (SVD).
+    The state of that study is drawn U[0, 1) by the caller."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = np.zeros((NOCTANT, nm, na))
+    m = np.zeros((NOCTANT, na, nm))
+    for o in range(NOCTANT):
+        A = rng.normal(0.0, 1.0 / np.sqrt(nm), size=(na, nm))  # [ia][im]
+        a[o] = A.T
+        m[o] = np.linalg.pinv(A).T
+    return a.reshape(-1), m.reshape(-1)
+
+
 class Problem:
     """One sweep problem driven through the reference-compatible C API:
     Env + Quantities (built-in) + Sweeper created from a reference flag string."""

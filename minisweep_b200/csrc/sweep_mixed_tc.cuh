@@ -736,7 +736,10 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         tmem_ld16(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32 + 16, d1);
         tmem_wait_ld();
         if (pe.act) {
-          const float f0 = f_pow2(-k2s[(pe.gg & 1) * 128 + row]), f1 = f_pow2(-pe.k2), fk = f_pow2(-kb2);
+          // un-scale in FP64: exact, and no intermediate can overflow (the
+          // scaled accumulators times 2^-k may exceed the FP32 range even
+          // where the result does not)
+          const double s0 = d_pow2(-k2s[(pe.gg & 1) * 128 + row] - kb2), s1 = d_pow2(-pe.k2 - kb2);
           const unsigned char* old = vo_ring + (size_t)slot * C::VBUF;
           double2 o[CH];
 #pragma unroll
@@ -744,10 +747,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             o[jj] = first ? make_double2(0.0, 0.0) : *reinterpret_cast<const double2*>(old + vswz<C>(row, jj));
 #pragma unroll
           for (int jj = 0; jj < CH; ++jj) {
-            const float t0 = __fmul_rn(__fmaf_rn(d1[2 * jj], f1, __fmul_rn(d0[2 * jj], f0)), fk);
-            const float t1 = __fmul_rn(__fmaf_rn(d1[2 * jj + 1], f1, __fmul_rn(d0[2 * jj + 1], f0)), fk);
-            o[jj].x = __dadd_rn(o[jj].x, (double)t0);
-            o[jj].y = __dadd_rn(o[jj].y, (double)t1);
+            o[jj].x = __dadd_rn(o[jj].x, __fma_rn((double)d0[2 * jj], s0, __dmul_rn((double)d1[2 * jj], s1)));
+            o[jj].y = __dadd_rn(o[jj].y, __fma_rn((double)d0[2 * jj + 1], s0, __dmul_rn((double)d1[2 * jj + 1], s1)));
           }
           double2* dst = reinterpret_cast<double2*>(pe.dst);
 #pragma unroll
@@ -790,7 +791,9 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         const float cxz = f_pow2(-2 - ((sp_xy - 3 * dy + 7 * iz) & 3));
         const float sx_r = f_pow2(-((sp_xy - dx + 7 * iz) & 3));
         const float cc = so_r * f_pow2((sp_xy + 7 * iz) & 3);
-        const float vsc1 = f_pow2(-k1), vsc2 = f_pow2(-kb1);  // two steps: each stays a normal float
+        // vs = D1 * 2^-(k1 + kb1) in two exact steps, the smaller factor first,
+        // so no intermediate leaves the FP32 range unless vs itself does
+        const float vsc1 = f_pow2(min(-k1, -kb1)), vsc2 = f_pow2(max(-k1, -kb1));
         const int prev = (int)((G - 1) & 1), cur = (int)(G & 1);
         float* out_slot = slots + ((size_t)((cur * TY + b) * 2 + half) * 32 + lane) * 16;
         float* gout_yz = x_out ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)EF + j * 32 : nullptr;
