@@ -50,6 +50,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
+// Non-blocking test of a phase (test_wait never suspends the warp).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // try_wait with a suspend-time hint: the warp sleeps in hardware until the
 // phase completes or about `ns` nanoseconds pass (no busy polling).
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity, uint32_t ns) {
@@ -67,6 +78,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity, uint
 // completed (the loader finishes the stages it issued and then posts a stop),
 // so only a time-out ends it early.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, const SyncArgs& s, int task) {
+  if (mbar_test_wait(b, parity)) return true;  // already complete: no suspension
   if (mbar_try_wait(b, parity, 20000)) return true;
   const long long t0 = global_ns();
   for (;;) {

@@ -123,6 +123,14 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -208,7 +216,10 @@ struct MixCfg {
   static constexpr int A2M = 128 * NA * 2;  // LBO 128, SBO 512
   static constexpr int B1M = NA * KP * 2;   // [angle][moment], LBO 128, SBO 256
   static constexpr int B2M = 16 * NA * 2;   // [moment][angle], LBO 128, SBO 512
-  static constexpr int MATBUF = 2 * B1M + 2 * B2M;
+  // B1 comes twice, with moments 8-15 and with moments 0-7 zeroed (the two
+  // halves of vi carry separate row scales: T1 is two products); then B2
+  static constexpr bool SPLIT_K = NM_ > 8;
+  static constexpr int MATBUF = 4 * B1M + 2 * B2M;
   static constexpr int SLOT = 32 * 16 * 4;  // one warp's outgoing faces (16 angles)
   // shared-memory layout (bytes)
   static constexpr int SM_STAGE = 0;
@@ -218,14 +229,15 @@ struct MixCfg {
   static constexpr int SM_MAT = SM_A2 + 2 * A2M;      // [2 buffers][B1 hi, B1 lo, B2 hi, B2 lo]
   static constexpr int SM_SLOT = SM_MAT + 2 * MATBUF;  // [2 parity][tile row][2 halves]
   static constexpr int SM_KS = SM_SLOT + 2 * TY * 2 * SLOT;  // row scales k1, k2: [2][2][128] ints
-  static constexpr int SM_BAR = SM_KS + 2 * 2 * 128 * 4;
+  static constexpr int SM_BAR = SM_KS + 2 * 2 * 2 * 128 * 4;
   // barriers: full, done, freed [NS]; d1, d2 [2]; fin; previous-vo ring [NRING]
   static constexpr int NBAR = 3 * NS + 2 * 2 + 1 + NRING;
   static constexpr int SM_MISC = SM_BAR + 8 * NBAR;  // tmem base, matrix scales [2][2]
   static constexpr size_t smem_bytes() { return (size_t)SM_MISC + 64; }
-  // tensor memory columns: D1 [2][32 angles], D2 [2][2 angle halves][16 moments]
-  static constexpr int TM_COLS = 128;
-  static constexpr int TM_D1 = 0, TM_D2 = 64;
+  // tensor memory columns: D1 [2 buffers][2 moment halves][32 angles],
+  // D2 [2 buffers][2 angle halves][16 moments]
+  static constexpr int TM_COLS = 256;
+  static constexpr int TM_D1 = 0, TM_D2 = 128;
 };
 
 // Byte offset of (row, 16-byte chunk jj) in a swizzled vi / vo block buffer.
@@ -295,13 +307,13 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
 
   // Named barriers.  1: the eight compute warps and the MMA warp, once per
   // step (A2, slots and row scales of the step complete) and at task starts;
-  // 2: the four vi converters arrive, the MMA warp waits (A1 complete).  A
+  // 2: the compute warps arrive, the MMA warp waits (A1 complete).  A
   // bounded mbarrier wait that runs out only raises s_abort; every warp reads
   // it after the next barrier 1 and they all leave together, so no warp is
   // ever left at a barrier.
   auto bar_step = []() { asm volatile("bar.sync 1, %0;" ::"n"((NW + 1) * 32) : "memory"); };
-  auto arrive_a1 = []() { asm volatile("bar.arrive 2, %0;" ::"n"((NW / 2 + 1) * 32) : "memory"); };
-  auto sync_a1 = []() { asm volatile("bar.sync 2, %0;" ::"n"((NW / 2 + 1) * 32) : "memory"); };
+  auto arrive_a1 = []() { asm volatile("bar.arrive 2, %0;" ::"n"((NW + 1) * 32) : "memory"); };
+  auto sync_a1 = []() { asm volatile("bar.sync 2, %0;" ::"n"((NW + 1) * 32) : "memory"); };
   auto wait = [&](uint64_t* bar, long long phase_index, int per) {
     if (!mbar_wait(bar, (uint32_t)((phase_index / per) & 1), P.sy, -1)) s_abort = 1;
   };
@@ -380,14 +392,18 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         }
         const int kb1 = split_scale_d(m1), kb2 = split_scale_d(m2);
         const double s1 = d_pow2(kb1), s2 = d_pow2(kb2);
-        // B1[angle][moment] = a_from_m[oct][moment][angle]
+        // B1[angle][moment] = a_from_m[oct][moment][angle]: B1a keeps moments
+        // 0-7 (all of them when NM <= 8), B1b moments 8-15
         for (int e = lane; e < C::NA * C::KP; e += 32) {
           const int n = e / C::KP, k = e % C::KP;
           const double x = (n < P.na && k < NM_) ? __ldg(&P.afm[n + (size_t)P.na * (k + (size_t)NM_ * oct)]) * s1 : 0.0;
           const uint16_t hi = H::rn(x), lo = H::rn(x - (double)H::val(hi));
           const int off = kmajor_off(n, k, 128, 256);
-          *reinterpret_cast<uint16_t*>(mat + off) = hi;
-          *reinterpret_cast<uint16_t*>(mat + C::B1M + off) = lo;
+          const bool in_a = k < 8 || !C::SPLIT_K;
+          *reinterpret_cast<uint16_t*>(mat + off) = in_a ? hi : (uint16_t)0;
+          *reinterpret_cast<uint16_t*>(mat + C::B1M + off) = in_a ? lo : (uint16_t)0;
+          *reinterpret_cast<uint16_t*>(mat + 2 * C::B1M + off) = in_a ? (uint16_t)0 : hi;
+          *reinterpret_cast<uint16_t*>(mat + 3 * C::B1M + off) = in_a ? (uint16_t)0 : lo;
         }
         // B2[moment][angle] = m_from_a[oct][angle][moment]
         for (int e = lane; e < 16 * C::NA; e += 32) {
@@ -395,8 +411,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
           const double x = (n < NM_ && k < P.na) ? __ldg(&P.mfa[n + (size_t)NM_ * (k + (size_t)P.na * oct)]) * s2 : 0.0;
           const uint16_t hi = H::rn(x), lo = H::rn(x - (double)H::val(hi));
           const int off = kmajor_off(n, k, 128, 512);
-          *reinterpret_cast<uint16_t*>(mat + 2 * C::B1M + off) = hi;
-          *reinterpret_cast<uint16_t*>(mat + 2 * C::B1M + C::B2M + off) = lo;
+          *reinterpret_cast<uint16_t*>(mat + 4 * C::B1M + off) = hi;
+          *reinterpret_cast<uint16_t*>(mat + 4 * C::B1M + C::B2M + off) = lo;
         }
         if (lane == 0) {
           mat_scale[2 * mb] = kb1;
@@ -540,13 +556,18 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
     // converters have written A1, T2 of step G at the end of step G.
     constexpr uint32_t ID1 = umma_idesc(FMT, 128, C::NA), ID2 = umma_idesc(FMT, 128, 16);
     const uint32_t a1u = smem_u32(smem + C::SM_A1), a2u = smem_u32(smem + C::SM_A2);
+    // the two moment halves of A1 carry separate row scales: one product and
+    // one accumulator each (B1a / B1b zero the other half's moments)
     auto issue_t1 = [&](long long gg, uint32_t b1) {
       tc_fence_after();
       if (lane == 0) {
-        const uint32_t d = tmem + C::TM_D1 + (uint32_t)(gg & 1) * 32;
-        umma_f16(d, umma_sdesc(a1u + C::A1M, 128, 256), umma_sdesc(b1, 128, 256), ID1, 0);  // lo x hi
-        umma_f16(d, umma_sdesc(a1u, 128, 256), umma_sdesc(b1 + C::B1M, 128, 256), ID1, 1);  // hi x lo
-        umma_f16(d, umma_sdesc(a1u, 128, 256), umma_sdesc(b1, 128, 256), ID1, 1);           // hi x hi
+#pragma unroll
+        for (int kh = 0; kh < (C::SPLIT_K ? 2 : 1); ++kh) {
+          const uint32_t d = tmem + C::TM_D1 + (uint32_t)(gg & 1) * 64 + 32u * kh, bb = b1 + 2 * C::B1M * kh;
+          umma_f16(d, umma_sdesc(a1u + C::A1M, 128, 256), umma_sdesc(bb, 128, 256), ID1, 0);  // lo x hi
+          umma_f16(d, umma_sdesc(a1u, 128, 256), umma_sdesc(bb + C::B1M, 128, 256), ID1, 1);  // hi x lo
+          umma_f16(d, umma_sdesc(a1u, 128, 256), umma_sdesc(bb, 128, 256), ID1, 1);           // hi x hi
+        }
         umma_commit(&d1bar[gg & 1]);
       }
       __syncwarp();
@@ -577,7 +598,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2, oct = hdr->oct, gp = hdr->gp;
       const bool first = (hdr->flags & TF_FIRST) != 0;
       const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
-      const uint32_t b1u = smem_u32(smem + C::SM_MAT + hdr->mat * C::MATBUF), b2u = b1u + 2 * C::B1M;
+      const uint32_t b1u = smem_u32(smem + C::SM_MAT + hdr->mat * C::MATBUF), b2u = b1u + 4 * C::B1M;
       const long long G0 = G;
       // The previous vo of step t (every cell of the tile, one TMA box each)
       // into ring slot (G0 + t) % NRING; the slot's last reader, the vo update
@@ -638,8 +659,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
     unsigned char* const a1s = smem + C::SM_A1;
     unsigned char* const a2s = smem + C::SM_A2;
     float* const slots = reinterpret_cast<float*>(smem + C::SM_SLOT);
-    int* const k1s = reinterpret_cast<int*>(smem + C::SM_KS);  // [2][128] row scale of A1
-    int* const k2s = k1s + 256;                                 // [2][128] row scale of A2, angles 0-15
+    int* const k1s = reinterpret_cast<int*>(smem + C::SM_KS);  // [2][moment half][128] row scales of A1
+    int* const k2s = k1s + 512;                                 // [2][angle half][128] row scales of A2
     const int sw = (lane >> 1) & 3;  // swizzle of the 64-byte slot rows
     float carry[16];
 #pragma unroll
@@ -683,41 +704,42 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
                           (size_t)(slab * P.ne) * (size_t)iz0;
       const long long zstep = (long long)(slab * P.ne) * dz;
 
-      // half 0: vi of global step gg (landed in its stage) -> scaled hi/lo row of A1
+      // vi of global step gg (landed in its stage) -> scaled hi/lo K-chunk
+      // `half` of this row of A1 (moments 8*half .. 8*half + 7, zero padded)
       auto convert_vi = [&](long long gg, bool act) {
         int k1 = 0;
-        if (act) {
+        uint32_t hi[4] = {0u, 0u, 0u, 0u}, lo[4] = {0u, 0u, 0u, 0u};
+        constexpr int M0 = 0;  // first moment of the chunk, relative to 8 * half
+        if (act && 8 * half < NM_) {
           const unsigned char* src = stages + (size_t)(gg % NS) * C::STAGE + C::ST_VI;
-          double v[NM_];
+          constexpr int NMC = NM_ < 8 ? NM_ : 8;  // moments in this chunk
+          double v[NMC];
 #pragma unroll
-          for (int jj = 0; jj < CH; ++jj) {
-            const double2 p = *reinterpret_cast<const double2*>(src + vswz<C>(row, jj));
+          for (int jj = 0; jj < NMC / 2; ++jj) {
+            const double2 p = *reinterpret_cast<const double2*>(src + vswz<C>(row, 4 * half + jj));
             v[2 * jj] = p.x;
             v[2 * jj + 1] = p.y;
           }
-          int emax = 0;  // largest biased exponent of the row
+          int emax = 0;  // largest biased exponent of the chunk
 #pragma unroll
-          for (int k = 0; k < NM_; ++k) emax = max(emax, (int)((__double_as_longlong(v[k]) >> 52) & 0x7ff));
+          for (int k = 0; k < NMC; ++k) emax = max(emax, (int)((__double_as_longlong(v[k]) >> 52) & 0x7ff));
           k1 = emax == 0 ? 0 : max(-120, min(120, 15 - (emax - 1022)));
           const double sc = d_pow2(k1);
-          uint32_t hi[C::KP / 2], lo[C::KP / 2];
 #pragma unroll
-          for (int p = 0; p < C::KP / 2; ++p) {
-            const float x0 = 2 * p < NM_ ? __double2float_rn(v[2 * p] * sc) : 0.0f;
-            const float x1 = 2 * p + 1 < NM_ ? __double2float_rn(v[2 * p + 1] * sc) : 0.0f;
+          for (int p = 0; p < 4; ++p) {
+            const float x0 = M0 + 2 * p < NMC ? __double2float_rn(v[2 * p < NMC ? 2 * p : 0] * sc) : 0.0f;
+            const float x1 = M0 + 2 * p + 1 < NMC ? __double2float_rn(v[2 * p + 1 < NMC ? 2 * p + 1 : 0] * sc) : 0.0f;
             hi[p] = H::pack(x0, x1);
             const float2 hv = H::unpack(hi[p]);
             lo[p] = H::pack(__fsub_rn(x0, hv.x), __fsub_rn(x1, hv.y));
           }
-#pragma unroll
-          for (int kc = 0; kc < C::KP / 8; ++kc) {
-            const int off = kmajor_off(row, 8 * kc, 128, 256);
-            *reinterpret_cast<uint4*>(a1s + off) = make_uint4(hi[4 * kc], hi[4 * kc + 1], hi[4 * kc + 2], hi[4 * kc + 3]);
-            *reinterpret_cast<uint4*>(a1s + C::A1M + off) =
-                make_uint4(lo[4 * kc], lo[4 * kc + 1], lo[4 * kc + 2], lo[4 * kc + 3]);
-          }
         }
-        k1s[(gg & 1) * 128 + row] = k1;
+        if (act) {
+          const int off = kmajor_off(row, 8 * half, 128, 256);
+          *reinterpret_cast<uint4*>(a1s + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+          *reinterpret_cast<uint4*>(a1s + C::A1M + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        }
+        k1s[(gg & 1) * 256 + half * 128 + row] = k1;
       };
       struct Pend {
         long long gg;
@@ -725,39 +747,43 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         int k2;
         bool act;
       };
-      // half 1: vo(gg) = [vo_old +] D2(gg) for this row (D2 complete: waited by the caller)
+      // vo(gg) = [vo_old +] D2(gg) for this row's moments of this half,
+      // 8*half .. (D2 complete: waited by the caller; the A2 scales of both
+      // angle halves were written before a barrier)
       auto epilogue = [&](const Pend& pe) {
-        // (the A2 scale of angles 0-15 was written by half 0 before a barrier)
+        constexpr int MH = NM_ / 2;  // moments per half
         const int slot = (int)(pe.gg % C::NRING);
         wait(&vobar[slot], pe.gg, C::NRING);
         tc_fence_after();
-        float d0[16], d1[16];
-        tmem_ld16(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32, d0);
-        tmem_ld16(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32 + 16, d1);
+        float d0[8], d1[8];
+        tmem_ld8(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32 + MH * half, d0);
+        tmem_ld8(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32 + 16 + MH * half, d1);
         tmem_wait_ld();
         if (pe.act) {
           // un-scale in FP64: exact, and no intermediate can overflow (the
           // scaled accumulators times 2^-k may exceed the FP32 range even
           // where the result does not)
-          const double s0 = d_pow2(-k2s[(pe.gg & 1) * 128 + row] - kb2), s1 = d_pow2(-pe.k2 - kb2);
+          const int kx = (pe.gg & 1) * 256 + row;
+          const double s0 = d_pow2(-k2s[kx] - kb2), s1 = d_pow2(-k2s[kx + 128] - kb2);
           const unsigned char* old = vo_ring + (size_t)slot * C::VBUF;
-          double2 o[CH];
+          constexpr int HC = MH / 2;  // 16-byte chunks per half row
+          double2 o[HC];
 #pragma unroll
-          for (int jj = 0; jj < CH; ++jj)
-            o[jj] = first ? make_double2(0.0, 0.0) : *reinterpret_cast<const double2*>(old + vswz<C>(row, jj));
+          for (int q = 0; q < HC; ++q)
+            o[q] = first ? make_double2(0.0, 0.0) : *reinterpret_cast<const double2*>(old + vswz<C>(row, HC * half + q));
 #pragma unroll
-          for (int jj = 0; jj < CH; ++jj) {
-            o[jj].x = __dadd_rn(o[jj].x, __fma_rn((double)d0[2 * jj], s0, __dmul_rn((double)d1[2 * jj], s1)));
-            o[jj].y = __dadd_rn(o[jj].y, __fma_rn((double)d0[2 * jj + 1], s0, __dmul_rn((double)d1[2 * jj + 1], s1)));
+          for (int q = 0; q < HC; ++q) {
+            o[q].x = __dadd_rn(o[q].x, __fma_rn((double)d0[2 * q], s0, __dmul_rn((double)d1[2 * q], s1)));
+            o[q].y = __dadd_rn(o[q].y, __fma_rn((double)d0[2 * q + 1], s0, __dmul_rn((double)d1[2 * q + 1], s1)));
           }
-          double2* dst = reinterpret_cast<double2*>(pe.dst);
+          double2* dst = reinterpret_cast<double2*>(pe.dst) + HC * half;
 #pragma unroll
-          for (int jj = 0; jj < CH; ++jj) dst[jj] = o[jj];
+          for (int q = 0; q < HC; ++q) dst[q] = o[q];
         }
       };
       // ---- prologue: vi of step 0 -> A1 (only cell (0, 0) is active), T1 of
       // step 0 issued; the previous vo of step 0 requested
-      if (half == 0) convert_vi(G0, rowv && cbeg == 0);
+      convert_vi(G0, rowv && cbeg == 0);
       fence_async_smem();
       tc_fence_before();
       bar_step();
@@ -771,9 +797,16 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         if (s > 0) wait(&full[st], G, NS);
         const int c = s - cbeg;
         const bool act = rowv && c >= 0 && c < nzr;
-        // ---- this step's T1 is done: D1 readable, A1 free for the next step
+        // ---- this step's T1 is done: D1 readable, A1 free for the next step.
+        // D1 is read before the next step's T1 is released: a TMEM load
+        // issued while an MMA runs waits for it.
         wait(&d1bar[G & 1], G, 2);
-        if (half == 0 && s + 1 < nsteps) {
+        tc_fence_after();
+        float v[16], vb[16];
+        tmem_ld16(trow + C::TM_D1 + (uint32_t)(G & 1) * 64 + 16 * half, v);
+        if constexpr (C::SPLIT_K) tmem_ld16(trow + C::TM_D1 + (uint32_t)(G & 1) * 64 + 32 + 16 * half, vb);
+        tmem_wait_ld();
+        if (s + 1 < nsteps) {
           // vi of the next step of this task: the loader's stage G + 1
           wait(&full[(G + 1) % NS], G + 1, NS);
           convert_vi(G + 1, rowv && c + 1 >= 0 && c + 1 < nzr);
@@ -781,19 +814,18 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
           tc_fence_before();
           arrive_a1();
         }
-        tc_fence_after();
-        float v[16];
-        tmem_ld16(trow + C::TM_D1 + (uint32_t)(G & 1) * 32 + 16 * half, v);
-        const int k1 = k1s[(G & 1) * 128 + row];
+        const int k1 = k1s[(G & 1) * 256 + row], k1b = k1s[(G & 1) * 256 + 128 + row];
 
         const int iz = iz0 + dz * c;
         const float cxy = f_pow2(-1 - ((sp_xy + 7 * (iz - dz)) & 3));
         const float cxz = f_pow2(-2 - ((sp_xy - 3 * dy + 7 * iz) & 3));
         const float sx_r = f_pow2(-((sp_xy - dx + 7 * iz) & 3));
         const float cc = so_r * f_pow2((sp_xy + 7 * iz) & 3);
-        // vs = D1 * 2^-(k1 + kb1) in two exact steps, the smaller factor first,
-        // so no intermediate leaves the FP32 range unless vs itself does
+        // vs = D1a * 2^-(k1 + kb1) [+ D1b * 2^-(k1b + kb1)], each term in two
+        // exact steps, the smaller factor first, so no intermediate leaves the
+        // FP32 range unless the term itself does
         const float vsc1 = f_pow2(min(-k1, -kb1)), vsc2 = f_pow2(max(-k1, -kb1));
+        const float vbs1 = f_pow2(min(-k1b, -kb1)), vbs2 = f_pow2(max(-k1b, -kb1));
         const int prev = (int)((G - 1) & 1), cur = (int)(G & 1);
         float* out_slot = slots + ((size_t)((cur * TY + b) * 2 + half) * 32 + lane) * 16;
         float* gout_yz = x_out ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)EF + j * 32 : nullptr;
@@ -850,7 +882,6 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             boundary((float)d_scale_space(ix, iy, gz), fxy);
           }
         }
-        tmem_wait_ld();
         // ---- Quantities_solve in FP32 (fused multiply-adds: fewer roundings)
         float pmax = 0.0f;
         if (act) {
@@ -860,7 +891,9 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             const float wz = 0.25f - 1.0f / (float)(1 << (ia & 7));
             const float sab = __fmaf_rn(fxy[i], cxy, __fmul_rn(fxz[i], cxz));
             const float sm = __fmaf_rn(fyz[i], __fmul_rn(wz, sx_r), sab);
-            const float psi = __fmaf_rn(sm, cc, __fmul_rn(__fmul_rn(v[i], vsc1), vsc2));
+            float vs = __fmul_rn(__fmul_rn(v[i], vsc1), vsc2);
+            if constexpr (C::SPLIT_K) vs = __fmaf_rn(__fmul_rn(vb[i], vbs1), vbs2, vs);
+            const float psi = __fmaf_rn(sm, cc, vs);
             v[i] = psi;
             pmax = fmaxf(pmax, fabsf(psi));
             carry[i] = __fmul_rn(psi, so);
@@ -888,7 +921,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             *reinterpret_cast<uint4*>(a2s + C::A2M + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
           }
         }
-        if (half == 0) k2s[(G & 1) * 128 + row] = k2;
+        k2s[(G & 1) * 256 + half * 128 + row] = k2;
         fence_async_smem();  // A2 rows before the MMA warp's T2 (issued after the step barrier)
         // ---- outgoing faces: the slot (next step's neighbours) and the tile's edges
         if (act) {
@@ -903,7 +936,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
           }
         }
         // ---- vo of the previous step (its products had this step to finish)
-        if (has_pend && half == 1) epilogue(pend);
+        if (has_pend) epilogue(pend);
         pend = Pend{G, act ? P.vo + (size_t)((long long)row0 + zstep * c) : nullptr, k2, act};
         has_pend = true;
         // ---- step barrier: A2 rows, slots and row scales of step G complete
@@ -913,7 +946,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         if (s == nsteps - 1) {
           // flush: the task's last vo before the task is reported complete
           wait(&d2bar[G & 1], G, 2);
-          if (half == 1) epilogue(pend);
+          epilogue(pend);
           tc_fence_before();
           bar_step();
           if (s_abort) { stop = true; break; }
