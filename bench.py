@@ -286,7 +286,8 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
         out.append({"precision": prec, "format": fmt[prec], "value": value, "unit": UNIT,
                     "ms_per_step": 1e3 * elapsed / args.steps, "ms_per_sweep_kernel": ms_sweep,
                     "dtype": "fp16/bf16 split products, fp32 accumulate and faces, f64 vo",
-                    "gpu_launches": args.steps * NITER, "clocks": clk,
+                    "gpu_launches": 2 * args.steps * NITER, "clocks": clk,
+                    "launches_per_sweep": "2: the sweep kernel and the FP64 sum of the eight octant partials",
                     "step": "%d sweeps of the initial state (not fed back: see error_note)" % NITER,
                     "error_builtin": {"max_rel": one_max, "normsq_rel": one_nsq},
                     "error_note": "errors of one sweep against the FP64 sweep of the same input; fed back, "

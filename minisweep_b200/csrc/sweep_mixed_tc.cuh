@@ -60,15 +60,17 @@
 
 namespace msb {
 
-// tm_vi / tm_vo describe the state array as a 5-D tensor (moment, NU * x,
-// y, group, z) for TMA tile copies of one cell: a box of NM moments x 4
-// unknowns x 1 x 2 groups x 1, swizzled so that rows read by consecutive
-// lanes fall in distinct banks.
+// tm_vi describes the state array as a 5-D tensor (moment, NU * x, y, group,
+// z) for TMA tile copies of one cell: a box of NM moments x 4 unknowns x 1 x 2
+// groups x 1, swizzled so that rows read by consecutive lanes fall in
+// distinct banks.  Each octant's contribution to vo is written to its own
+// FP32 partial array (the state layout, `part + oct * state`); a second
+// kernel sums the eight partials into vo in FP64.
 struct MixParams {
   CUtensorMap tm_vi;
-  CUtensorMap tm_vo;
   const double* vi;
-  double* vo;
+  float* part;
+  size_t state;  // elements of one state array
   const double* afm;  // a_from_m [oct][im][ia]
   const double* mfa;  // m_from_a [oct][ia][im]
   float* fxy;         // face planes: one 1 KiB entry per (octant, group pair, position)
@@ -201,7 +203,6 @@ struct MixCfg {
   static constexpr int VCELL = 8 * VROW;  // bytes of one box (alignment of its destination)
   static constexpr int VBUF = 128 * VROW;
   static constexpr int SWM = NM_ == 16 ? 7 : NM_ == 8 ? 3 : 1;
-  static constexpr int NRING = 2;  // previous-vo ring
   // stage (bytes), filled by the loader with bulk copies: entering yz faces
   // (one per tile row), xz (one per column), xy of the first plane (one per
   // row), vi of every cell column at this step, then the step header
@@ -223,15 +224,14 @@ struct MixCfg {
   static constexpr int SLOT = 32 * 16 * 4;  // one warp's outgoing faces (16 angles)
   // shared-memory layout (bytes)
   static constexpr int SM_STAGE = 0;
-  static constexpr int SM_VO = SM_STAGE + NS * STAGE;
-  static constexpr int SM_A1 = SM_VO + NRING * VBUF;  // [hi, lo]
+  static constexpr int SM_A1 = SM_STAGE + NS * STAGE;  // [hi, lo]
   static constexpr int SM_A2 = SM_A1 + 2 * A1M;       // [hi, lo]
   static constexpr int SM_MAT = SM_A2 + 2 * A2M;      // [2 buffers][B1 hi, B1 lo, B2 hi, B2 lo]
   static constexpr int SM_SLOT = SM_MAT + 2 * MATBUF;  // [2 parity][tile row][2 halves]
   static constexpr int SM_KS = SM_SLOT + 2 * TY * 2 * SLOT;  // row scales k1, k2: [2][2][128] ints
   static constexpr int SM_BAR = SM_KS + 2 * 2 * 2 * 128 * 4;
-  // barriers: full, done, freed [NS]; d1, d2 [2]; fin; previous-vo ring [NRING]
-  static constexpr int NBAR = 3 * NS + 2 * 2 + 1 + NRING;
+  // barriers: full, done, freed [NS]; d1, d2 [2]; fin
+  static constexpr int NBAR = 3 * NS + 2 * 2 + 1;
   static constexpr int SM_MISC = SM_BAR + 8 * NBAR;  // tmem base, matrix scales [2][2]
   static constexpr size_t smem_bytes() { return (size_t)SM_MISC + 64; }
   // tensor memory columns: D1 [2 buffers][2 moment halves][32 angles],
@@ -267,7 +267,6 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
   uint64_t* const d1bar = freed + NS;  // T1 of step G done (tcgen05.commit)
   uint64_t* const d2bar = d1bar + 2;    // T2 of step G done
   uint64_t* const finbar = d2bar + 2;
-  uint64_t* const vobar = finbar + 1;  // [NRING]
   uint32_t* const tmem_base = reinterpret_cast<uint32_t*>(smem + C::SM_MISC);
   int* const mat_scale = reinterpret_cast<int*>(smem + C::SM_MISC + 16);  // [2][kb1, kb2]
   __shared__ volatile int s_final;
@@ -289,7 +288,6 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       mbar_init(&d2bar[i], 1);
     }
     mbar_init(finbar, 1);
-    for (int i = 0; i < C::NRING; ++i) mbar_init(&vobar[i], 1);
     s_final = -1;
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -594,31 +592,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       if (s_abort) break;
       const StepHdr* hdr = reinterpret_cast<const StepHdr*>(stages + (size_t)(G % NS) * C::STAGE + C::ST_HDR);
       if (hdr->stop) break;
-      const int x0 = hdr->x0, x1 = hdr->x1, y0 = hdr->y0, y1 = hdr->y1, z0 = hdr->z0, z1 = hdr->z1;
-      const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2, oct = hdr->oct, gp = hdr->gp;
-      const bool first = (hdr->flags & TF_FIRST) != 0;
-      const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
+      const int nsteps = (hdr->z1 - hdr->z0) + (hdr->x1 - hdr->x0) + (hdr->y1 - hdr->y0) - 2;
       const uint32_t b1u = smem_u32(smem + C::SM_MAT + hdr->mat * C::MATBUF), b2u = b1u + 4 * C::B1M;
-      const long long G0 = G;
-      // The previous vo of step t (every cell of the tile, one TMA box each)
-      // into ring slot (G0 + t) % NRING; the slot's last reader, the vo update
-      // of step G0 + t - NRING, finished before the barrier that precedes this.
-      // Every step is requested exactly once (zero bytes for a first visit).
-      auto fetch_vo = [&](int t) {
-        const long long gt = G0 + t;
-        const int slot = (int)(gt % C::NRING);
-        const int a2 = lane & 3, b2 = lane >> 2, cv = t - a2 - b2;
-        const bool ok = !first && lane < TX * TY && a2 < w && b2 < h && cv >= 0 && cv < nzr;
-        const uint32_t bytes = (uint32_t)__popc(__ballot_sync(0xffffffffu, ok)) * P.vbox_bytes;
-        if (lane == 0) mbar_arrive_expect_tx(&vobar[slot], bytes);
-        __syncwarp();
-        if (ok) {
-          const int ix2 = dx > 0 ? x0 + a2 : x1 - 1 - a2, iy2 = dy > 0 ? y0 + b2 : y1 - 1 - b2;
-          tma_load_5d(smem + C::SM_VO + (size_t)slot * C::VBUF + (4 * b2 + a2) * C::VCELL, &P.tm_vo, 0, NU * ix2, iy2,
-                      2 * gp, dz > 0 ? z0 + cv : z1 - 1 - cv, &vobar[slot]);
-        }
-      };
-      fetch_vo(0);
       bar_step();  // A1 of the task's first step written
       if (s_abort) break;
       issue_t1(G, b1u);
@@ -632,7 +607,6 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         if (s_abort) { quit = true; break; }
         issue_t2(G, b2u);
         if (s > 0 && lane == 0) mbar_arrive(&done[(G - 1) % NS]);  // vo of step G - 1 written
-        if (s + 1 < nsteps) fetch_vo(s + 1);
         if (s == nsteps - 1) {
           bar_step();  // the task's last vo written
           if (s_abort) { quit = true; break; }
@@ -655,7 +629,6 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
     const int row = 32 * b + lane;
     const int ia0 = 16 * half;
     const uint32_t trow = tmem + ((uint32_t)(32 * b) << 16);
-    unsigned char* const vo_ring = smem + C::SM_VO;
     unsigned char* const a1s = smem + C::SM_A1;
     unsigned char* const a2s = smem + C::SM_A2;
     float* const slots = reinterpret_cast<float*>(smem + C::SM_SLOT);
@@ -679,7 +652,6 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const int x0 = hdr0->x0, x1 = hdr0->x1, y0 = hdr0->y0, y1 = hdr0->y1, z0 = hdr0->z0, z1 = hdr0->z1;
       const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2;
       const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
-      const bool first = (flags & TF_FIRST) != 0;
       const int g_col = 2 * gp + g;
       const bool rowv = a < w && b < h && g_col < P.ne;  // this row exists in the task
       const int ix = dx > 0 ? x0 + a : x1 - 1 - a;
@@ -703,6 +675,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const size_t row0 = (size_t)NM_ * u + (size_t)NM_ * NU * (ix + (size_t)P.nx * iy) + slab * (size_t)g_col +
                           (size_t)(slab * P.ne) * (size_t)iz0;
       const long long zstep = (long long)(slab * P.ne) * dz;
+      float* const part_oct = P.part + P.state * (size_t)oct;
 
       // vi of global step gg (landed in its stage) -> scaled hi/lo K-chunk
       // `half` of this row of A1 (moments 8*half .. 8*half + 7, zero padded)
@@ -743,17 +716,16 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       };
       struct Pend {
         long long gg;
-        double* dst;
+        float* dst;
         int k2;
         bool act;
       };
-      // vo(gg) = [vo_old +] D2(gg) for this row's moments of this half,
-      // 8*half .. (D2 complete: waited by the caller; the A2 scales of both
-      // angle halves were written before a barrier)
+      // this octant's contribution D2(gg) to vo, this row's moments of this
+      // half (8*half ..), into the octant's FP32 partial array (D2 complete:
+      // waited by the caller; the A2 scales of both angle halves were written
+      // before a barrier)
       auto epilogue = [&](const Pend& pe) {
         constexpr int MH = NM_ / 2;  // moments per half
-        const int slot = (int)(pe.gg % C::NRING);
-        wait(&vobar[slot], pe.gg, C::NRING);
         tc_fence_after();
         float d0[8], d1[8];
         tmem_ld8(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32 + MH * half, d0);
@@ -764,21 +736,22 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
           // scaled accumulators times 2^-k may exceed the FP32 range even
           // where the result does not)
           const int kx = (pe.gg & 1) * 256 + row;
+          // un-scaled in FP64 (exact; no intermediate can overflow), rounded
+          // once to FP32
           const double s0 = d_pow2(-k2s[kx] - kb2), s1 = d_pow2(-k2s[kx + 128] - kb2);
-          const unsigned char* old = vo_ring + (size_t)slot * C::VBUF;
-          constexpr int HC = MH / 2;  // 16-byte chunks per half row
-          double2 o[HC];
+          float o[MH];
 #pragma unroll
-          for (int q = 0; q < HC; ++q)
-            o[q] = first ? make_double2(0.0, 0.0) : *reinterpret_cast<const double2*>(old + vswz<C>(row, HC * half + q));
+          for (int m = 0; m < MH; ++m)
+            o[m] = __double2float_rn(__fma_rn((double)d0[m], s0, __dmul_rn((double)d1[m], s1)));
+          float* dst = pe.dst + MH * half;
+          if constexpr (MH % 4 == 0) {
 #pragma unroll
-          for (int q = 0; q < HC; ++q) {
-            o[q].x = __dadd_rn(o[q].x, __fma_rn((double)d0[2 * q], s0, __dmul_rn((double)d1[2 * q], s1)));
-            o[q].y = __dadd_rn(o[q].y, __fma_rn((double)d0[2 * q + 1], s0, __dmul_rn((double)d1[2 * q + 1], s1)));
+            for (int q = 0; q < MH / 4; ++q)
+              reinterpret_cast<float4*>(dst)[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < MH / 2; ++q) reinterpret_cast<float2*>(dst)[q] = make_float2(o[2 * q], o[2 * q + 1]);
           }
-          double2* dst = reinterpret_cast<double2*>(pe.dst) + HC * half;
-#pragma unroll
-          for (int q = 0; q < HC; ++q) dst[q] = o[q];
         }
       };
       // ---- prologue: vi of step 0 -> A1 (only cell (0, 0) is active), T1 of
@@ -937,7 +910,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         }
         // ---- vo of the previous step (its products had this step to finish)
         if (has_pend) epilogue(pend);
-        pend = Pend{G, act ? P.vo + (size_t)((long long)row0 + zstep * c) : nullptr, k2, act};
+        pend = Pend{G, act ? part_oct + (size_t)((long long)row0 + zstep * c) : nullptr, k2, act};
         has_pend = true;
         // ---- step barrier: A2 rows, slots and row scales of step G complete
         tc_fence_before();
@@ -963,6 +936,28 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
   tc_fence_after();
   if (warp == NW + 2)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TM_COLS) : "memory");
+}
+
+// vo = sum over the eight octants of their FP32 partials, in FP64 and in
+// octant order (deterministic).  n is a multiple of 4 (NM * NU elements per
+// (cell, group)).
+__global__ void __launch_bounds__(256) reduce_octant_partials(double* __restrict__ vo,
+                                                              const float* __restrict__ part, size_t n) {
+  const size_t n4 = n / 4;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+    for (int o = 0; o < NOCTANT; ++o) {
+      const float4 q = __ldcs(reinterpret_cast<const float4*>(part + n * o) + i);
+      a0 = __dadd_rn(a0, (double)q.x);
+      a1 = __dadd_rn(a1, (double)q.y);
+      a2 = __dadd_rn(a2, (double)q.z);
+      a3 = __dadd_rn(a3, (double)q.w);
+    }
+    double2* d = reinterpret_cast<double2*>(vo) + 2 * i;
+    __stcs(d, make_double2(a0, a1));
+    __stcs(d + 1, make_double2(a2, a3));
+  }
 }
 
 }  // namespace msb

@@ -174,10 +174,13 @@ struct SweeperImpl {
   size_t face_bytes[3] = {0, 0, 0};
   double* d_afm = nullptr;
   double* d_mfa = nullptr;
+  float* d_part = nullptr;  // mixed precision: FP32 partial vo per octant
+  size_t part_elems = 0;
   double* d_vi = nullptr;  // staging for host-only Pointers
   double* d_vo = nullptr;
   long long timeout_ns = kDefaultTimeoutNs;
   int nlaunch = 0;
+  int nsm = 0;
   int* h_status = nullptr;  // pinned copy of the status words
 
   ~SweeperImpl() {
@@ -186,6 +189,7 @@ struct SweeperImpl {
     for (auto& f : d_face) cudaFree(f);
     cudaFree(d_afm);
     cudaFree(d_mfa);
+    cudaFree(d_part);
     cudaFree(d_vi);
     cudaFree(d_vo);
     if (h_status) cudaFreeHost(h_status);
@@ -227,6 +231,11 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision) {
   S.face_bytes[2] = per * dims.ncell_z * dims.ncell_y;
   for (int f = 0; f < 3; ++f)
     if ((rc = cuda_check(cudaMalloc(&S.d_face[f], S.face_bytes[f]), "cudaMalloc faces"))) return rc;
+  if (S.var.mix) {
+    S.part_elems = (size_t)NOCTANT * Dimensions_size_state(dims, NU);
+    if ((rc = cuda_check(cudaMalloc(&S.d_part, S.part_elems * sizeof(float)), "cudaMalloc octant partials")))
+      return rc;
+  }
   const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
   if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
   if ((rc = cuda_check(cudaMalloc(&S.d_mfa, nmat * sizeof(double)), "cudaMalloc m_from_a"))) return rc;
@@ -241,6 +250,7 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision) {
     return rc;
   if (occ < 1) return set_error(MSB_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
   S.grid = (int)std::min<long long>(ntask, (long long)nsm * occ);
+  S.nsm = nsm;
   return MSB_OK;
 }
 
@@ -268,7 +278,6 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
   auto fill = [&](auto& P, auto* face) {
     using F = std::remove_pointer_t<decltype(face)>;
     P.vi = vi_d;
-    P.vo = vo_d;
     P.afm = S.d_afm;
     P.mfa = S.d_mfa;
     P.fxy = static_cast<F*>(S.d_face[0]);
@@ -288,19 +297,23 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
   if (S.var.fn) {
     Fp64Params P;
     fill(P, (double*)nullptr);
+    P.vo = vo_d;
     S.var.fn<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
   } else {
     MixParams P;
     fill(P, (float*)nullptr);
+    P.part = S.d_part;
+    P.state = S.part_elems / NOCTANT;
     if ((rc = encode_state_map(&P.tm_vi, vi_d, S.dims, &P.vbox_bytes))) return rc;
-    if ((rc = encode_state_map(&P.tm_vo, vo_d, S.dims, &P.vbox_bytes))) return rc;
     S.var.mix<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
+    if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
+    reduce_octant_partials<<<S.nsm * 8, 256, 0, stream>>>(vo_d, S.d_part, P.state);
   }
   if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
                        "status copy")))
     return rc;
-  S.nlaunch = 1;
+  S.nlaunch = S.var.mix ? 2 : 1;
   return MSB_OK;
 }
 
