@@ -13,6 +13,10 @@ the built-in problem and on the random-input study (state U[0,1) from
 torch's generator seeded 1234, a_from_m N(0, 1/nm) from PCG64 seed 1234,
 m_from_a its pseudo-inverse).
 
+`batched` reports the batched serving workload beside them: 256 independent
+problems of uneven sizes (seed 7) swept by one persistent launch per sweep,
+with problems/s and the per-problem completion latency (p50 / p99).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Under torchrun each rank sweeps its own 64-group slice (energy groups are
@@ -303,6 +307,115 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
     return out
 
 
+def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict | None:
+    """The batched serving workload: 256 independent problems (seed 7, sizes in
+    msb.batch_workload), every one swept by ONE persistent launch per sweep;
+    under torchrun each rank takes every world-th problem (no exchange).
+    Reports problems/s, the per-problem completion latency inside the launch
+    (p50 / p99), the CUDA-graph iteration loop, and the same problems swept
+    one Sweeper at a time for comparison."""
+    if args.no_batch:
+        return None
+    import numpy as np
+    import torch
+
+    import minisweep_b200 as msb
+    from minisweep_b200.parallel import max_over_ranks
+
+    W = msb.batch_workload()
+    mine = [i for i in range(len(W)) if i % world == rank]
+    probs = [W[i] for i in mine]
+    vis, vos, mats, descs = [], [], {}, []
+    for q in probs:
+        n = msb.state_size(q)
+        vi = torch.empty(n, dtype=torch.float64, device=dev)
+        vo = torch.empty_like(vi)
+        msb.init_state_device(vi.data_ptr(), q)
+        key = (q["nm"], q["na"])
+        if key not in mats:
+            a, m = msb.builtin_matrices(*key)
+            mats[key] = (torch.from_numpy(a).to(dev), torch.from_numpy(m).to(dev))
+        vis.append(vi)
+        vos.append(vo)
+        descs.append(dict(q, vi=vi.data_ptr(), vo=vo.data_ptr(), a_from_m=mats[key][0].data_ptr(),
+                          m_from_a=mats[key][1].data_ptr()))
+    torch.cuda.synchronize()
+    t0 = time.time()
+    b = msb.Batch(descs, autotune=True)
+    create_s = time.time() - t0
+    info = b.info()
+    s = torch.cuda.Stream(device=dev)
+    sh = s.cuda_stream
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        b.sync(sh)
+        return e0.elapsed_time(e1)
+
+    for _ in range(max(1, args.batch_warmup)):
+        b.sweep(0, sh)
+        b.sync(sh)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    ms = [timed(lambda: b.sweep(0, sh)) for _ in range(max(1, args.batch_steps))]
+    clk = clocks.stop()
+    done_ms = b.problem_ms()
+    graph_ms = timed(lambda: b.run(2, sh))  # vi -> vo -> vi as one captured graph
+    b.sweep(0, sh)
+    b.sync(sh)
+    b.close()
+    # the same problems, one Sweeper (one launch) after another
+    seq_ms = 0.0
+    exact = True
+    for i, q in enumerate(probs):
+        fl = f"--ncell_x {q['ncell_x']} --ncell_y {q['ncell_y']} --ncell_z {q['ncell_z']} --ne {q['ne']} --na {q['na']}"
+        with msb.Problem(fl, nm=q["nm"]) as pb1:
+            ref = torch.empty_like(vos[i]) if i < 8 else vos[i]
+            st1 = torch.cuda.ExternalStream(pb1.stream) if pb1.stream else torch.cuda.current_stream()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st1)
+            pb1.sweep_device(ref.data_ptr(), vis[i].data_ptr())
+            e1.record(st1)
+            pb1.sync()
+            seq_ms += e0.elapsed_time(e1)
+            if i < 8:  # the batched result equals the problem's own Sweeper bit for bit
+                exact = exact and bool(torch.equal(ref, vos[i]))
+    batch_ms = max_over_ranks(min(ms) / 1e3) * 1e3
+    seq_ms = max_over_ranks(seq_ms / 1e3) * 1e3
+    upd = sum(q["ncell_x"] * q["ncell_y"] * q["ncell_z"] * q["ne"] * q["na"] * 8 for q in W)
+    del vis, vos, descs, mats
+    torch.cuda.empty_cache()
+    return {"workload": "batched serving: 256 independent problems from seed 7 (numpy PCG64), ncell_x,y in "
+                        "{8..48}, ncell_z in {8..64}, ne in {8,16,32,64}, na in {16,32,64}, NM in {4,16}, NU 4, "
+                        "built-in Quantities, FP64",
+            "metric": "problems/s", "value": len(W) / (batch_ms / 1e3), "unit": "problems/s",
+            "updates_per_s": upd / (batch_ms / 1e3),
+            "ms_per_batch_sweep": batch_ms, "launches_per_sweep": 1,
+            "latency_ms": {"p50": float(np.percentile(done_ms, 50)), "p99": float(np.percentile(done_ms, 99)),
+                           "max": float(done_ms.max()),
+                           "definition": "device time from the start of the batched launch to the completion "
+                                         "of each problem's last task (rank 0's share)"},
+            "graph_2_iterations_ms": graph_ms,
+            "unbatched_ms": seq_ms,
+            "speedup_vs_unbatched": seq_ms / batch_ms,
+            "exact_vs_sweeper": exact,
+            "problems_per_rank": len(probs), "ntask": info["ntask"],
+            "classes": [{"nm": c["nm"], "angle_chunks": c["nch"], "tile": list(c["tile"]), "ntask": c["ntask"]}
+                        for c in info["classes"]],
+            "scratch_gb": info["scratch_bytes"] / 1e9, "scratch_needed_all_gb": info["scratch_needed_all"] / 1e9,
+            "scratch_waits": info["npred"], "create_s": create_s, "autotune_ms": info["tune_ms"],
+            "clocks": clk,
+            "note": "one persistent launch sweeps every problem; the face scratch of all problems at once "
+                    "does not fit beside the state, so problems reuse the scratch of completed ones (device-side "
+                    "waits on per-problem completion counters)"}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     import torch
 
@@ -380,6 +493,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
         pass
 
     def finish(e2e):
+        pb.close()
+        batched = measure_batched(args, dev, world, rank, local_rank)
         upd = updates_per_sweep() * NITER
         value = upd * args.steps * world / elapsed
         ms_sweep = sum(sweep_ms) / len(sweep_ms)
@@ -423,9 +538,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                                     "against it",
                     "check": {"normsq": normsq, "normsqdiff": normsqdiff, "normsq_closed_form": closed,
                               "pass": normsqdiff == 0.0 and (closed is None or normsq == closed)},
-                    "ms_per_sweep_kernel": ms_sweep}
+                    "ms_per_sweep_kernel": ms_sweep,
+                    "batched": batched}
             print(json.dumps(line), flush=True)
-        pb.close()
         if dist is not None:
             dist.destroy_process_group()
         return 0
@@ -465,6 +580,9 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched serving workload")
+    ap.add_argument("--batch-steps", type=int, default=2, help="timed batched sweeps")
+    ap.add_argument("--batch-warmup", type=int, default=1, help="untimed batched sweeps")
     ap.add_argument("--case", choices=["config2", "small"], default="config2",
                     help="small: 32^3 cells, ne 32, one sweep per step, no e2e / CPU legs (profiling runs)")
     args = ap.parse_args()
@@ -474,6 +592,7 @@ def main() -> int:
         NE, NITER = 32, 1
         args.no_cpu = True
         args.no_e2e = True
+        args.no_batch = True
         WORKLOAD = WORKLOAD.replace("64x64x64", "32x32x32").replace("ne 64", "ne 32").replace(
             "niterations 10", "niterations 1")
     else:

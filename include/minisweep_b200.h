@@ -367,6 +367,81 @@ int msb_measure_fp64_peak(double* tflops_dmma, double* tflops_dfma, int reps);
 int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double* a_from_m_d, const double* m_from_a_d,
                       int ncell_x, int ncell_y, int ncell_z, int ne, int nm, int na, void* stream);
 
+/*---------------------------------------------------------------- batches
+ * Many independent sweep problems in one persistent kernel launch.  No
+ * counterpart in the reference, which sweeps one problem per Sweeper
+ * (Sweeper_create, sweeper_kba_c.h:44-287; Sweeper_sweep, :588-845); a batch
+ * sweeps every problem exactly as that problem's own Sweeper would (FP64, the
+ * built-in or the caller's transform matrices), with results identical bit
+ * for bit.
+ *
+ * Each problem has its own sizes (nm 4, 8 or 16; na <= 64) and its own device
+ * arrays in the reference layouts: vi/vo the state (16-byte aligned),
+ * a_from_m [octant][im][ia] and m_from_a [octant][ia][im].  The face planes
+ * are scratch from one device arena of scratch_bytes (0: what all problems
+ * need at once, capped at 80 % of the free device memory); problems that do
+ * not fit at once reuse the bytes of problems that completed earlier in the
+ * same launch.  autotune != 0 times the two tile shapes (4 x 2 and 2 x 4
+ * cells) on the median problem of each (nm, angle chunk) group at creation;
+ * those trial sweeps write that problem's vo.  Asynchronous calls run on the
+ * given stream (a cudaStream_t, NULL = the legacy default stream); their
+ * device status is checked by msb_batch_sync. */
+typedef struct {
+  int ncell_x, ncell_y, ncell_z, ne, na, nm;
+  double* vi;               /* input of even sweeps (dir 0) */
+  double* vo;               /* output of even sweeps        */
+  const double* a_from_m;
+  const double* m_from_a;
+} msb_problem;
+typedef struct msb_batch msb_batch;
+enum { MSB_BATCH_MAX_CLASSES = 16 };
+typedef struct {
+  int nproblem, nclass, npred, nsm;
+  long long ntask;
+  size_t scratch_bytes;       /* arena size                              */
+  size_t scratch_needed_all;  /* face scratch of all problems at once    */
+  double sim_makespan;        /* planner's simulated time (relative units) */
+  double sim_busy;            /* planner's simulated SM utilisation (0-1)  */
+  double tune_ms;             /* time spent in autotuning trial sweeps   */
+  int class_nm[MSB_BATCH_MAX_CLASSES], class_nch[MSB_BATCH_MAX_CLASSES];
+  int class_tx[MSB_BATCH_MAX_CLASSES], class_ty[MSB_BATCH_MAX_CLASSES];
+  long long class_ntask[MSB_BATCH_MAX_CLASSES];
+} msb_batch_info_t;
+/* precision must be 0 (FP64). */
+int msb_batch_create(msb_batch** out, const msb_problem* problems, int nproblem, int precision,
+                     size_t scratch_bytes, int autotune);
+void msb_batch_destroy(msb_batch* b);
+/* One launch: every problem sweeps vo = sweep(vi) (dir 0) or vi = sweep(vo)
+ * (dir 1). */
+int msb_batch_sweep(msb_batch* b, int dir, void* stream);
+/* The reference driver's iteration loop (runner.c:148-155) for every problem:
+ * niterations sweeps alternating dir 0 and 1 (the result of the last sweep is
+ * in vo for an odd count, in vi for an even one), launched as one CUDA graph
+ * captured on the first call with this count. */
+int msb_batch_run(msb_batch* b, int niterations, void* stream);
+int msb_batch_sync(msb_batch* b, void* stream);
+/* Per problem: ms from the start of the last launch to the completion of the
+ * problem's last task (device clock).  After msb_batch_sync. */
+int msb_batch_problem_ms(const msb_batch* b, double* ms, int n);
+int msb_batch_info(const msb_batch* b, msb_batch_info_t* info);
+/* Host-only planning of the same batch for nsm SMs (no device, pointers may
+ * be NULL) for host-side checks; bit (3 * (nch - 1) + k) of tile24_mask, k = 0,
+ * 1, 2 for nm 4, 8, 16, selects the 2 x 4 tile for that group. */
+int msb_batch_plan(msb_batch** out, const msb_problem* problems, int nproblem, int nsm,
+                   size_t scratch_bytes, int tile24_mask);
+/* The planned task table (global ids, MSB_TASK_INTS ints per task) and the
+ * problem of each task; returns the task count. */
+long long msb_batch_tasks(const msb_batch* b, int* rec, int* prob, long long max_tasks);
+/* Arena placement per problem (offset, bytes) and the problems each one waits
+ * for (pred[pred_off[p] .. pred_off[p + 1])); returns the predecessor count. */
+int msb_batch_scratch(const msb_batch* b, long long* offset, long long* bytes, int* pred_off, int* pred,
+                      int max_pred);
+/* Test hook: time budget (ns) of every device wait; 0 = default (4 s). */
+int msb_batch_set_spin_limit(msb_batch* b, long long limit);
+/* The built-in transform matrices (Quantities_init_am_matrices_,
+ * quantities_testing_c.h:40-201) for nm moments and na angles, 8 octants. */
+int msb_builtin_matrices(int nm, int na, double* a_from_m, double* m_from_a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,27 @@ class Sweeper(ctypes.Structure):
             "nthread_y", "nthread_z", "is_face_comm_async", "precision")] + [("impl_", ctypes.c_void_p)]
 
 
+class ProblemDesc(ctypes.Structure):
+    """msb_problem: one problem of a batch (sizes + device arrays)."""
+    _fields_ = [("ncell_x", ctypes.c_int), ("ncell_y", ctypes.c_int), ("ncell_z", ctypes.c_int),
+                ("ne", ctypes.c_int), ("na", ctypes.c_int), ("nm", ctypes.c_int),
+                ("vi", ctypes.c_void_p), ("vo", ctypes.c_void_p),
+                ("a_from_m", ctypes.c_void_p), ("m_from_a", ctypes.c_void_p)]
+
+
+MAX_CLASSES = 16
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("nproblem", ctypes.c_int), ("nclass", ctypes.c_int), ("npred", ctypes.c_int),
+                ("nsm", ctypes.c_int), ("ntask", ctypes.c_longlong), ("scratch_bytes", ctypes.c_size_t),
+                ("scratch_needed_all", ctypes.c_size_t), ("sim_makespan", ctypes.c_double),
+                ("sim_busy", ctypes.c_double), ("tune_ms", ctypes.c_double),
+                ("class_nm", ctypes.c_int * MAX_CLASSES), ("class_nch", ctypes.c_int * MAX_CLASSES),
+                ("class_tx", ctypes.c_int * MAX_CLASSES), ("class_ty", ctypes.c_int * MAX_CLASSES),
+                ("class_ntask", ctypes.c_longlong * MAX_CLASSES)]
+
+
 _lib = None
 
 
@@ -100,6 +121,23 @@ def lib() -> ctypes.CDLL:
         L.msb_initialize_state_device.argtypes = [ctypes.c_void_p, Dimensions, P(Env)]
         L.msb_schedule_tasks.argtypes = [ctypes.c_int] * 7 + [P(ctypes.c_int), ctypes.c_longlong]
         L.msb_schedule_tasks.restype = ctypes.c_longlong
+        L.msb_batch_create.argtypes = [P(ctypes.c_void_p), P(ProblemDesc), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_size_t, ctypes.c_int]
+        L.msb_batch_plan.argtypes = [P(ctypes.c_void_p), P(ProblemDesc), ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_size_t, ctypes.c_int]
+        L.msb_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.msb_batch_destroy.restype = None
+        L.msb_batch_sweep.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.msb_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.msb_batch_sync.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.msb_batch_problem_ms.argtypes = [ctypes.c_void_p, P(D), ctypes.c_int]
+        L.msb_batch_info.argtypes = [ctypes.c_void_p, P(BatchInfo)]
+        L.msb_batch_tasks.argtypes = [ctypes.c_void_p, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_longlong]
+        L.msb_batch_tasks.restype = ctypes.c_longlong
+        L.msb_batch_scratch.argtypes = [ctypes.c_void_p, P(ctypes.c_longlong), P(ctypes.c_longlong),
+                                        P(ctypes.c_int), P(ctypes.c_int), ctypes.c_int]
+        L.msb_batch_set_spin_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+        L.msb_builtin_matrices.argtypes = [ctypes.c_int, ctypes.c_int, P(D), P(D)]
         L.initialize_state.argtypes = [P(D), Dimensions, ctypes.c_int, P(Quantities)]
         L.get_state_norms.argtypes = [P(D), P(D), Dimensions, ctypes.c_int, P(D), P(D), P(Env)]
         _lib = L
@@ -268,3 +306,137 @@ class Problem:
 
     def __exit__(self, *exc):
         self.close()
+
+
+# ------------------------------------------------------------------ batches
+def batch_workload(n: int = 256, seed: int = 7) -> list:
+    """The batched serving workload: n independent problems drawn with numpy's
+    PCG64 from `seed`, in this order per field: ncell_x and ncell_y uniform in
+    {8..48}, ncell_z in {8..64}, ne from {8, 16, 32, 64}, na from {16, 32, 64},
+    nm from {4, 16} (NU = 4, built-in Quantities)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nx = rng.integers(8, 49, n)
+    ny = rng.integers(8, 49, n)
+    nz = rng.integers(8, 65, n)
+    ne = rng.choice([8, 16, 32, 64], n)
+    na = rng.choice([16, 32, 64], n)
+    nm = rng.choice([4, 16], n)
+    return [dict(ncell_x=int(nx[i]), ncell_y=int(ny[i]), ncell_z=int(nz[i]), ne=int(ne[i]), na=int(na[i]),
+                 nm=int(nm[i])) for i in range(n)]
+
+
+def state_size(p: dict) -> int:
+    return p["ncell_x"] * p["ncell_y"] * p["ncell_z"] * p["ne"] * p["nm"] * NU
+
+
+def init_state_device(v_ptr: int, p: dict) -> None:
+    """Built-in initial state of problem p into a device array (default stream)."""
+    d = Dimensions(p["ncell_x"], p["ncell_y"], p["ncell_z"], p["ne"], p["nm"], p["na"])
+    _check(lib().msb_initialize_state_device(ctypes.c_void_p(v_ptr), d, None))
+
+
+def builtin_matrices(nm: int, na: int):
+    """Built-in a_from_m / m_from_a (reference layouts) for nm moments, na angles."""
+    n = nm * na * NOCTANT
+    a, m = np.zeros(n), np.zeros(n)
+    DP = ctypes.POINTER(ctypes.c_double)
+    _check(lib().msb_builtin_matrices(nm, na, a.ctypes.data_as(DP), m.ctypes.data_as(DP)))
+    return a, m
+
+
+def _descs(problems: list):
+    arr = (ProblemDesc * len(problems))()
+    for i, p in enumerate(problems):
+        arr[i] = ProblemDesc(p["ncell_x"], p["ncell_y"], p["ncell_z"], p["ne"], p["na"], p["nm"],
+                             p.get("vi", 0) or None, p.get("vo", 0) or None, p.get("a_from_m", 0) or None,
+                             p.get("m_from_a", 0) or None)
+    return arr
+
+
+class Batch:
+    """Many problems swept by one persistent kernel launch (msb_batch_*).
+
+    `problems`: dicts with the sizes (ncell_x, ncell_y, ncell_z, ne, na, nm)
+    and device pointers (vi, vo, a_from_m, m_from_a).  With `plan_nsm` set,
+    only the host-side plan is built (no GPU; pointers may be absent)."""
+
+    def __init__(self, problems: list, precision: int = 0, scratch_bytes: int = 0, autotune: bool = False,
+                 plan_nsm: int = 0, tile24_mask: int = 0):
+        L = lib()
+        self.n = len(problems)
+        self._h = ctypes.c_void_p()
+        d = _descs(problems)
+        if plan_nsm:
+            rc = L.msb_batch_plan(ctypes.byref(self._h), d, self.n, plan_nsm, scratch_bytes, tile24_mask)
+        else:
+            rc = L.msb_batch_create(ctypes.byref(self._h), d, self.n, precision, scratch_bytes, int(autotune))
+        _check(rc)
+
+    def sweep(self, direction: int = 0, stream: int = 0) -> None:
+        _check(lib().msb_batch_sweep(self._h, direction, ctypes.c_void_p(stream)))
+
+    def run(self, niterations: int, stream: int = 0) -> None:
+        _check(lib().msb_batch_run(self._h, niterations, ctypes.c_void_p(stream)))
+
+    def sync(self, stream: int = 0) -> None:
+        _check(lib().msb_batch_sync(self._h, ctypes.c_void_p(stream)))
+
+    def problem_ms(self) -> np.ndarray:
+        out = np.zeros(self.n)
+        _check(lib().msb_batch_problem_ms(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.n))
+        return out
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        _check(lib().msb_batch_info(self._h, ctypes.byref(i)))
+        nc = i.nclass
+        return dict(nproblem=i.nproblem, nclass=nc, npred=i.npred, nsm=i.nsm, ntask=i.ntask,
+                    scratch_bytes=i.scratch_bytes, scratch_needed_all=i.scratch_needed_all,
+                    sim_makespan=i.sim_makespan, sim_busy=i.sim_busy, tune_ms=i.tune_ms,
+                    classes=[dict(nm=i.class_nm[c], nch=i.class_nch[c], tile=(i.class_tx[c], i.class_ty[c]),
+                                  ntask=i.class_ntask[c]) for c in range(nc)])
+
+    def tasks(self):
+        """(table: ntask x 16 ints with global dependency ids, problem of each task)."""
+        L = lib()
+        n = L.msb_batch_tasks(self._h, None, None, 0)
+        rec = np.zeros((n, TASK_INTS), dtype=np.int32)
+        prob = np.zeros(n, dtype=np.int32)
+        IP = ctypes.POINTER(ctypes.c_int)
+        L.msb_batch_tasks(self._h, rec.ctypes.data_as(IP), prob.ctypes.data_as(IP), n)
+        return rec, prob
+
+    def scratch(self):
+        """(offset, bytes, pred_off, pred) of the face-scratch arena placement."""
+        L = lib()
+        off = np.zeros(self.n, dtype=np.int64)
+        nb = np.zeros(self.n, dtype=np.int64)
+        po = np.zeros(self.n + 1, dtype=np.int32)
+        LP, IP = ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)
+        npred = L.msb_batch_scratch(self._h, off.ctypes.data_as(LP), nb.ctypes.data_as(LP), po.ctypes.data_as(IP),
+                                    None, 0)
+        if npred < 0:
+            raise SweepError(npred, last_error())
+        pred = np.zeros(max(npred, 1), dtype=np.int32)
+        _check(min(0, L.msb_batch_scratch(self._h, None, None, None, pred.ctypes.data_as(IP), len(pred))))
+        return off, nb, po, pred[:npred]
+
+    def set_timeout_ns(self, ns: int) -> None:
+        _check(lib().msb_batch_set_spin_limit(self._h, ns))
+
+    def close(self) -> None:
+        if self._h:
+            lib().msb_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -266,21 +266,21 @@ extern "C" int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double*
   if ((rc = cuda_check(cudaMemsetAsync(sync, 0, sync_b, st), "clear progress"))) return rc;
 
   Fp64Params P;
-  P.vi = vi_d;
-  P.vo = vo_d;
-  P.afm = a_from_m_d;
-  P.mfa = m_from_a_d;
-  P.fxy = reinterpret_cast<double*>(base + sync_b + task_b);
-  P.fxz = reinterpret_cast<double*>(base + sync_b + task_b + fxy_b);
-  P.fyz = reinterpret_cast<double*>(base + sync_b + task_b + fxy_b + fxz_b);
+  P.pr.vi = vi_d;
+  P.pr.vo = vo_d;
+  P.pr.afm = a_from_m_d;
+  P.pr.mfa = m_from_a_d;
+  P.pr.fxy = reinterpret_cast<double*>(base + sync_b + task_b);
+  P.pr.fxz = reinterpret_cast<double*>(base + sync_b + task_b + fxy_b);
+  P.pr.fyz = reinterpret_cast<double*>(base + sync_b + task_b + fxy_b + fxz_b);
   P.tasks = tasks;
   P.ntask = ntask;
-  P.nx = ncell_x;
-  P.ny = ncell_y;
-  P.nz = ncell_z;
-  P.ne = ne;
-  P.na = na;
-  P.ngp = ngp;
+  P.pr.nx = ncell_x;
+  P.pr.ny = ncell_y;
+  P.pr.nz = ncell_z;
+  P.pr.ne = ne;
+  P.pr.na = na;
+  P.pr.ngp = ngp;
   P.sy.sync = sync;
   P.sy.timeout_ns = 4000000000LL;
   const int v = nm == 16 ? 1 : 0;

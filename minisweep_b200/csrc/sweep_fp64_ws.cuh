@@ -48,7 +48,8 @@
 
 namespace msb {
 
-struct Fp64Params {
+// One sweep problem as the kernel sees it.
+struct Fp64Prob {
   const double* vi;
   double* vo;
   const double* afm;  // a_from_m [oct][im][ia] (im stride nm)
@@ -56,11 +57,52 @@ struct Fp64Params {
   double* fxy;        // face planes, one entry = one warp's 8 columns x angles
   double* fxz;
   double* fyz;
+  int nx, ny, nz, ne, na, ngp;
+};
+
+// One problem per launch.
+struct Fp64Params {
+  Fp64Prob pr;
   const int* tasks;
   long long ntask;
-  int nx, ny, nz, ne, na, ngp;
   SyncArgs sy;
 };
+
+// Many problems per launch.  Tasks of all problems share one table with
+// global task ids; the problems are grouped in classes (moment count, angle
+// chunks, tile shape), each class a contiguous range of the table that the
+// CTAs work through in class order.  A problem whose face planes reuse the
+// scratch of earlier problems waits until those have completed every task.
+constexpr int kMaxBatchClasses = 16;
+struct Fp64Batch {
+  const int* tasks;       // MSB_TASK_INTS ints per task, dependencies as global ids
+  const int* task_prob;   // problem of each task
+  const Fp64Prob* probs;  // per problem, for direction 0 (vi -> vo)
+  const int* pred_off;    // scratch predecessors of problem p: pred[pred_off[p] .. pred_off[p + 1])
+  const int* pred;
+  const int* prob_ntask;  // tasks per problem
+  int* pdone;             // completed tasks per problem (zeroed before the launch)
+  long long* ptime;       // %globaltimer when each problem completed; [nprob] = launch start
+  long long cls_base[kMaxBatchClasses];
+  long long cls_ntask[kMaxBatchClasses];
+  int cls_kind[kMaxBatchClasses];
+  int nclass, nprob;
+  int dir;  // 1: every problem sweeps vo -> vi (the iteration loop's odd sweeps)
+  SyncArgs sy;
+};
+// First sync slot of the per-class task counters of a batched launch.
+constexpr int SY_CLASS0 = 4;
+static_assert(SY_CLASS0 + kMaxBatchClasses <= SY_PROGRESS, "sync header");
+
+__device__ __forceinline__ int atom_add_release(int* p, int v) {
+  int old;
+  asm volatile("atom.add.release.gpu.global.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t* b) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(b)) : "memory");
+}
 
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -98,11 +140,41 @@ struct Fp64Cfg {
   static constexpr int SM_STAGE = 4 * NW * ENT;
   static constexpr int SM_MAT = SM_STAGE + NS * STAGE;  // [2][MAT]
   static constexpr int SM_BAR = SM_MAT + 2 * MAT;       // full[NS], done[NS], freed[NS]
-  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)(SM_BAR + 3 * NS); }
+  static constexpr int SM_FINAL = SM_BAR + 3 * NS;      // loader -> publisher: steps issued (int)
+  static constexpr int SM_PROB = SM_FINAL + 1;          // batched: Fp64Prob of the task in each mat buffer
+  static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)SM_PROB; }
+  static constexpr size_t smem_bytes_batch() { return sizeof(double) * (size_t)SM_PROB + 2 * sizeof(Fp64Prob); }
 };
 
-template <int NM_, int NCH, int TX, int TY, int NS, bool PIPE_T1>
-__global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const Fp64Params P) {
+// Shared-memory barriers of one body: set up before its first stage, and
+// invalidated before another body reuses the memory.
+template <int NM_, int NCH, int TX, int TY, int NS>
+__device__ __forceinline__ void fp64_barriers(bool init) {
+  using C = Fp64Cfg<NM_, NCH, TX, TY, NS>;
+  extern __shared__ __align__(128) double smem[];
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + C::SM_BAR);
+  if (init) {
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(&bars[i], 1);            // full: the loader's arrive.expect_tx (header + face copies)
+      mbar_init(&bars[NS + i], C::NW);   // done: every compute warp
+      mbar_init(&bars[2 * NS + i], 1);   // freed: the publisher
+    }
+    *reinterpret_cast<volatile int*>(smem + C::SM_FINAL) = -1;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  } else {
+    for (int i = 0; i < 3 * NS; ++i) mbar_inval(&bars[i]);
+  }
+}
+
+// The sweep of one class of tasks by one CTA.  ROLE 0: the whole CTA (sets
+// up its barriers, then splits into the producer warpgroup and the compute
+// warps, moving registers from the first to the second); ROLE 1: the
+// producer warps only; ROLE 2: the compute warps only (a batched kernel
+// splits the roles once and sets up the barriers of each class itself).
+// BATCH: P is an Fp64Batch and `cls` the class whose table range this call
+// works through; otherwise P is an Fp64Params.
+template <int NM_, int NCH, int TX, int TY, int NS, bool PIPE_T1, bool BATCH, int ROLE, class PP>
+__device__ __forceinline__ void fp64_body(const PP& P, int cls) {
   using C = Fp64Cfg<NM_, NCH, TX, TY, NS>;
   constexpr int KS = C::KS, MT = C::MT, NW = C::NW, ENT = C::ENT, VSZ = C::VSZ;
   static_assert(NM_ % 4 == 0 && NM_ <= 16, "NM must be 4, 8 or 16");
@@ -115,27 +187,21 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
   uint64_t* const done = full + NS;
   uint64_t* const freed = done + NS;  // publisher consumed the step: loader may refill the stage
 
+  Fp64Prob* const s_prob = reinterpret_cast<Fp64Prob*>(smem + C::SM_PROB);  // BATCH only
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int* const sync = P.sy.sync;
   int* const progress = sync + SY_PROGRESS;
-  const size_t slab = (size_t)NM_ * NU * P.nx * P.ny;  // one (iz, ie) layer of the state
-  // loader <-> publisher hand-off (shared memory)
-  __shared__ volatile int s_final;      // total steps issued, once the loader stops (-1 before)
+  // loader <-> publisher hand-off: total steps issued, once the loader stops (-1 before)
+  volatile int& s_final = *reinterpret_cast<volatile int*>(smem + C::SM_FINAL);
 
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < NS; ++i) {
-      mbar_init(&full[i], 1);  // the loader's arrive.expect_tx (header + face copies)
-      mbar_init(&done[i], NW);
-      mbar_init(&freed[i], 1);
-    }
-    s_final = -1;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  if constexpr (ROLE == 0) {
+    if (threadIdx.x == 0) fp64_barriers<NM_, NCH, TX, TY, NS>(true);
+    __syncthreads();
   }
-  __syncthreads();
 
-  if (warp >= NW) {
+  if (ROLE == 1 || (ROLE == 0 && warp >= NW)) {
     // ====================================================== producer warpgroup
-    if constexpr (C::REBALANCE) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(C::REG_PRODUCER));
+    if constexpr (C::REBALANCE && ROLE == 0) asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(C::REG_PRODUCER));
     if (warp == NW) {
       // ------------------------------------------------------------ loader
       long long g_load = 0;
@@ -173,8 +239,13 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       auto grab = [&]() -> int {
         int t = -1;
         if (lane == 0 && ld_relaxed(&sync[SY_ABORT]) == 0) {
-          const long long tt = atomicAdd(&sync[SY_COUNTER], 1);
-          t = tt < P.ntask ? (int)tt : -1;
+          if constexpr (BATCH) {
+            const long long tt = atomicAdd(&sync[SY_CLASS0 + cls], 1);
+            t = tt < P.cls_ntask[cls] ? (int)(P.cls_base[cls] + tt) : -1;
+          } else {
+            const long long tt = atomicAdd(&sync[SY_COUNTER], 1);
+            t = tt < P.ntask ? (int)tt : -1;
+          }
         }
         return __shfl_sync(0xffffffffu, t, 0);
       };
@@ -197,8 +268,27 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
         const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
         const int depx = (mode & DM_X_PLANE) ? rec[TK_DEP_X] : -1;
         const int depy = (mode & DM_Y_PLANE) ? rec[TK_DEP_Y] : -1;
+        // the task's problem
+        Fp64Prob Q;
+        int prob = 0;
+        if constexpr (BATCH) {
+          prob = __ldg(&P.task_prob[t]);
+          Q = P.probs[prob];
+          if (P.dir) {
+            const double* a = Q.vi;
+            Q.vi = Q.vo;
+            Q.vo = const_cast<double*>(a);
+          }
+          // the face scratch is free once its previous users completed
+          for (int k = __ldg(&P.pred_off[prob]), ke = __ldg(&P.pred_off[prob + 1]); k < ke && !failed; ++k) {
+            const int q2 = __ldg(&P.pred[k]);
+            if (wait_dep(&P.pdone[q2], __ldg(&P.prob_ntask[q2]), t) < 0) failed = true;
+          }
+        } else {
+          Q = P.pr;
+        }
         // cross-phase dependencies: whole task complete
-        if (rec[TK_DEP_X] >= 0 && depx < 0 && wait_dep(&progress[rec[TK_DEP_X]], kComplete, t) < 0) failed = true;
+        if (!failed && rec[TK_DEP_X] >= 0 && depx < 0 && wait_dep(&progress[rec[TK_DEP_X]], kComplete, t) < 0) failed = true;
         if (!failed && rec[TK_DEP_Y] >= 0 && depy < 0 && wait_dep(&progress[rec[TK_DEP_Y]], kComplete, t) < 0) failed = true;
         if (!failed && rec[TK_DEP_Z] >= 0 && wait_dep(&progress[rec[TK_DEP_Z]], kComplete, t) < 0) failed = true;
         if (!failed && rec[TK_DEP_VO] >= 0 && wait_dep(&progress[rec[TK_DEP_VO]], kComplete, t) < 0) failed = true;
@@ -211,20 +301,23 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
         for (int e = lane; e < NCH * KS * 4 * 32; e += 32) {
           const int ln = e & 31, tt = (e >> 5) & 3, k = (e >> 7) % KS, ch = (e >> 7) / KS;
           const int ia = 32 * ch + 8 * tt + (ln >> 2), im = KS * (ln & 3) + k;
-          mat[e] = ia < P.na ? __ldg(&P.afm[ia + (size_t)P.na * (im + (size_t)NM_ * oct)]) : 0.0;
+          mat[e] = ia < Q.na ? __ldg(&Q.afm[ia + (size_t)Q.na * (im + (size_t)NM_ * oct)]) : 0.0;
         }
         for (int e = lane; e < NCH * MT * 8 * 32; e += 32) {
           const int ln = e & 31, i = (e >> 5) & 1, tt = (e >> 6) & 3, mt = (e >> 8) % MT, ch = (e >> 8) / MT;
           const int ia = 32 * ch + 8 * tt + 2 * (ln & 3) + i, im = 8 * mt + (ln >> 2);
           mat[NCH * KS * 4 * 32 + e] =
-              (ia < P.na && im < NM_) ? __ldg(&P.mfa[im + (size_t)NM_ * (ia + (size_t)P.na * oct)]) : 0.0;
+              (ia < Q.na && im < NM_) ? __ldg(&Q.mfa[im + (size_t)NM_ * (ia + (size_t)Q.na * oct)]) : 0.0;
+        }
+        if constexpr (BATCH) {
+          if (lane == 0) s_prob[mb] = Q;  // published to the compute warps with the task's first stage
         }
         __syncwarp();
         ++ntask_seen;
         last_step[mb] = g_load + nsteps - 1;
 
-        const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
-        const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;
+        const size_t ent_z = (size_t)(oct * Q.ngp + gp) * Q.nz;
+        const size_t ent_y = (size_t)(oct * Q.ngp + gp) * Q.ny;
         int seen_x = 0, seen_y = 0;  // progress of the upwind tiles already observed
         for (int s = 0; s < nsteps; ++s) {
           const int st = (int)(g_load % NS);
@@ -258,7 +351,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
           if (lane == 0) {
             hdr->task = t; hdr->s = s; hdr->oct = oct; hdr->gp = gp;
             hdr->x0 = x0; hdr->x1 = x1; hdr->y0 = y0; hdr->y1 = y1; hdr->z0 = z0; hdr->z1 = z1;
-            hdr->flags = flags; hdr->mat = mb; hdr->stop = 0;
+            hdr->flags = flags; hdr->mat = mb; hdr->stop = 0; hdr->pad1 = prob;
             // progress this task reaches once step s is done (-2: nothing new)
             hdr->pad0 = s == nsteps - 1 ? kComplete : (s + 1 - (w + h - 2) > 0 ? s + 1 - (w + h - 2) : -2);
             mbar_arrive_expect_tx(&full[st], bytes);
@@ -271,19 +364,19 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
               const int b = pos, c = s - b;
               if (c >= 0 && c < nzr) {
                 const int iy = dy > 0 ? y0 + b : y1 - 1 - b, iz = dz > 0 ? z0 + c : z1 - 1 - c;
-                bulk_g2s(stg + C::ST_YZ + b * ENT, P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT, ENT * 8, &full[st]);
+                bulk_g2s(stg + C::ST_YZ + b * ENT, Q.fyz + ((ent_z + iz) * Q.ny + iy) * (size_t)ENT, ENT * 8, &full[st]);
               }
             } else if (kind == 1 && pos < w && (flags & TF_Y_IN)) {
               const int a = pos, c = s - a;
               if (c >= 0 && c < nzr) {
                 const int ix = dx > 0 ? x0 + a : x1 - 1 - a, iz = dz > 0 ? z0 + c : z1 - 1 - c;
-                bulk_g2s(stg + C::ST_XZ + a * ENT, P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT, ENT * 8, &full[st]);
+                bulk_g2s(stg + C::ST_XZ + a * ENT, Q.fxz + ((ent_z + iz) * Q.nx + ix) * (size_t)ENT, ENT * 8, &full[st]);
               }
             } else if (kind == 2 && pos < h && (flags & TF_Z_IN)) {
               const int b = pos, a = s - b;
               if (a >= 0 && a < w) {
                 const int ix = dx > 0 ? x0 + a : x1 - 1 - a, iy = dy > 0 ? y0 + b : y1 - 1 - b;
-                bulk_g2s(stg + C::ST_XY + b * ENT, P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT, ENT * 8, &full[st]);
+                bulk_g2s(stg + C::ST_XY + b * ENT, Q.fxy + ((ent_y + iy) * Q.nx + ix) * (size_t)ENT, ENT * 8, &full[st]);
               }
             }
           }
@@ -304,6 +397,14 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
           hdr->stop = 1;
           mbar_arrive_expect_tx(&full[st], 0);
         }
+      } else {
+        // the compute warps stopped early (a wait ran out): let this warp's
+        // copies into the stages land before the shared memory is reused or
+        // released; a copy takes microseconds, the bound is 1 ms
+        const long long t1 = global_ns();
+        for (long long x = freed_upto + 1; x < g_load; ++x)
+          while (!mbar_test_wait(&full[x % NS], (uint32_t)((x / NS) & 1)) && global_ns() - t1 < 1000000) {
+          }
       }
       __syncwarp();
     } else if (warp == NW + 1) {
@@ -329,20 +430,22 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
           }
         }
         if (!ready) break;
-        int pend_task[2] = {-1, -1}, pend_val[2] = {-2, -2};
+        int pend_task[2] = {-1, -1}, pend_val[2] = {-2, -2}, pend_prob[2] = {0, 0};
         for (;;) {  // consume step G and any later steps already done
           const int st = (int)(G % NS);
           const StepHdr* hdr = reinterpret_cast<const StepHdr*>(stages + (size_t)st * C::STAGE + C::ST_HDR);
-          const int task = hdr->task, val = hdr->pad0;
+          const int task = hdr->task, val = hdr->pad0, hprob = hdr->pad1;
           __syncwarp();
           if (lane == 0) mbar_arrive(&freed[st]);
           if (val != -2) {
             if (pend_task[1] >= 0 && pend_task[1] != task) {
               pend_task[0] = pend_task[1];
               pend_val[0] = pend_val[1];
+              pend_prob[0] = pend_prob[1];
             }
             pend_task[1] = task;
             pend_val[1] = val;
+            pend_prob[1] = hprob;
           }
           ++G;
           // a task boundary ends a batch so older tasks are published first
@@ -356,14 +459,22 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
           if (lane == 0) {
             if (pend_task[0] >= 0) st_release(&progress[pend_task[0]], pend_val[0]);
             if (pend_task[1] >= 0) st_release(&progress[pend_task[1]], pend_val[1]);
+            if constexpr (BATCH) {
+              // a problem is complete once all its tasks are: the last one
+              // stamps the time and releases its face scratch to later problems
+              for (int k = 0; k < 2; ++k)
+                if (pend_task[k] >= 0 && pend_val[k] == kComplete) {
+                  const int pr2 = pend_prob[k];
+                  if (atom_add_release(&P.pdone[pr2], 1) + 1 == __ldg(&P.prob_ntask[pr2])) P.ptime[pr2] = global_ns();
+                }
+            }
           }
         }
         t0 = global_ns();
       }
     }
-    return;
-  }
-  if constexpr (C::REBALANCE) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(C::REG_COMPUTE));
+  } else {
+  if constexpr (C::REBALANCE && ROLE == 0) asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(C::REG_COMPUTE));
 
   // ================================================================ compute
   const int q = lane >> 2, r = lane & 3;
@@ -391,6 +502,13 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
     const int oct = hdr0->oct, gp = hdr0->gp, flags = hdr0->flags;
     const int x0 = hdr0->x0, x1 = hdr0->x1, y0 = hdr0->y0, y1 = hdr0->y1, z0 = hdr0->z0, z1 = hdr0->z1;
     const double* mat = mats + hdr0->mat * C::MAT;
+    // the task's problem: the launch's own, or (batched) the loader's copy in
+    // shared memory, read where used rather than held in registers
+    Fp64Prob Qv;
+    const Fp64Prob* qp = &Qv;
+    if constexpr (BATCH) qp = s_prob + hdr0->mat; else Qv = P.pr;
+    const Fp64Prob& Q = *qp;
+    const size_t slab = (size_t)NM_ * NU * Q.nx * Q.ny;  // one (iz, ie) layer of the state
     const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2;
     const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
     const bool first = (flags & TF_FIRST) != 0;
@@ -400,9 +518,9 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
     const int iz0 = dz > 0 ? z0 : z1 - 1;  // z of plane 0; plane c is iz0 + dz * c
     const int cbeg = wa + wb;              // step of this warp's plane 0
     const int g_col = 2 * gp + (q >> 2);
-    const bool gval = g_col < P.ne;
+    const bool gval = g_col < Q.ne;
     const int g_vo = 2 * gp + (r >> 1);
-    const bool gvo = g_vo < P.ne;
+    const bool gvo = g_vo < Q.ne;
     const double so = (double)(1 + oct);
     const double so_r = 1.0 / so;  // rounded, as the reference's 1/(1+octant)
     // boundary flux = (1+ia) 2^(ia&7) s_space s_energy s_unknown (1+oct):
@@ -410,10 +528,10 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
     const double face_k = gval ? (double)d_scale_energy(g_col) * (double)d_scale_unknown(q & 3) * so : 0.0;
     const int sp_xy = ix + 3 * iy + 2;  // log2 s_space(x, y, z) = (sp_xy + 7 z) & 3
     // state offsets (doubles) of this column: + zstep per plane
-    const size_t col = (size_t)NM_ * NU * (ix + (size_t)P.nx * iy);
-    const long long zstep = (long long)slab * P.ne * dz;
-    const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
-    const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;
+    const size_t col = (size_t)NM_ * NU * (ix + (size_t)Q.nx * iy);
+    const long long zstep = (long long)slab * Q.ne * dz;
+    const size_t ent_z = (size_t)(oct * Q.ngp + gp) * Q.nz;
+    const size_t ent_y = (size_t)(oct * Q.ngp + gp) * Q.ny;
     // edges of the tile that read or write global faces
     const bool x_in = wa == 0 && (flags & TF_X_IN), y_in = wb == 0 && (flags & TF_Y_IN);
     const bool z_in = (flags & TF_Z_IN) != 0;
@@ -439,14 +557,14 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
       const int c2 = s2 - cbeg;
       if (act && s2 < nsteps && c2 >= 0 && c2 < nzr) {
         double* dst = stages + (size_t)(G2 % NS) * C::STAGE + warp * VSZ;
-        const size_t off0 = col + slab * (size_t)(2 * gp) + (size_t)(slab * P.ne) * (size_t)(iz0 + dz * c2);
+        const size_t off0 = col + slab * (size_t)(2 * gp) + (size_t)(slab * Q.ne) * (size_t)(iz0 + dz * c2);
 #pragma unroll
         for (int g2 = 0; g2 < 2; ++g2) {
-          if (2 * gp + g2 >= P.ne) continue;
+          if (2 * gp + g2 >= Q.ne) continue;
 #pragma unroll
           for (int o = lane * 2; o < VSZ / 2; o += 64) {
-            cp_async16(dst + C::ST_VI + g2 * (VSZ / 2) + o, P.vi + off0 + g2 * slab + o);
-            if (!first) cp_async16(dst + C::ST_VO + g2 * (VSZ / 2) + o, P.vo + off0 + g2 * slab + o);
+            cp_async16(dst + C::ST_VI + g2 * (VSZ / 2) + o, Q.vi + off0 + g2 * slab + o);
+            if (!first) cp_async16(dst + C::ST_VO + g2 * (VSZ / 2) + o, Q.vo + off0 + g2 * slab + o);
           }
         }
       }
@@ -496,18 +614,18 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
         // where the three incoming faces come from
         const double* in_yz = wa > 0 ? slot_yz + (size_t)(prev * NW + warp - 1) * ENT
                               : (x_in && C::FACE_PF) ? stg + C::ST_YZ + wb * ENT : nullptr;
-        const double* gin_yz = (!C::FACE_PF && x_in) ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT : nullptr;
+        const double* gin_yz = (!C::FACE_PF && x_in) ? Q.fyz + ((ent_z + iz) * Q.ny + iy) * (size_t)ENT : nullptr;
         const double* in_xz = wb > 0 ? slot_xz + (size_t)(prev * NW + warp - TX) * ENT
                               : (y_in && C::FACE_PF) ? stg + C::ST_XZ + wa * ENT : nullptr;
-        const double* gin_xz = (!C::FACE_PF && y_in) ? P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT : nullptr;
+        const double* gin_xz = (!C::FACE_PF && y_in) ? Q.fxz + ((ent_z + iz) * Q.nx + ix) * (size_t)ENT : nullptr;
         const double* in_xy = (c == 0 && z_in && C::FACE_PF) ? stg + C::ST_XY + wb * ENT : nullptr;
-        const double* gin_xy = (c == 0 && z_in && !C::FACE_PF) ? P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT : nullptr;
+        const double* gin_xy = (c == 0 && z_in && !C::FACE_PF) ? Q.fxy + ((ent_y + iy) * Q.nx + ix) * (size_t)ENT : nullptr;
         double* out_yz = slot_yz + (size_t)(cur * NW + warp) * ENT;
         double* out_xz = slot_xz + (size_t)(cur * NW + warp) * ENT;
-        double* gout_yz = x_out ? P.fyz + ((ent_z + iz) * P.ny + iy) * (size_t)ENT : nullptr;
-        double* gout_xz = y_out ? P.fxz + ((ent_z + iz) * P.nx + ix) * (size_t)ENT : nullptr;
-        double* gout_xy = (c == nzr - 1 && z_out) ? P.fxy + ((ent_y + iy) * P.nx + ix) * (size_t)ENT : nullptr;
-        const int gx = dx > 0 ? -1 : P.nx, gy = dy > 0 ? -1 : P.ny, gz = dz > 0 ? -1 : P.nz;  // ghost cells
+        double* gout_yz = x_out ? Q.fyz + ((ent_z + iz) * Q.ny + iy) * (size_t)ENT : nullptr;
+        double* gout_xz = y_out ? Q.fxz + ((ent_z + iz) * Q.nx + ix) * (size_t)ENT : nullptr;
+        double* gout_xy = (c == nzr - 1 && z_out) ? Q.fxy + ((ent_y + iy) * Q.nx + ix) * (size_t)ENT : nullptr;
+        const int gx = dx > 0 ? -1 : Q.nx, gy = dy > 0 ? -1 : Q.ny, gz = dz > 0 ? -1 : Q.nz;  // ghost cells
 
         const bool has_next = PIPE_T1 && c + 1 < nzr;
         double vin[KS];
@@ -545,7 +663,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int ia = 32 * ch + 8 * t + 2 * r + i;
-                fyz[i] = ia < P.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(gx, iy, iz)) * face_k : 0.0;
+                fyz[i] = ia < Q.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(gx, iy, iz)) * face_k : 0.0;
               }
             }
             if (in_xz) {
@@ -558,7 +676,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int ia = 32 * ch + 8 * t + 2 * r + i;
-                fxz[i] = ia < P.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, gy, iz)) * face_k : 0.0;
+                fxz[i] = ia < Q.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, gy, iz)) * face_k : 0.0;
               }
             }
             if (c > 0) {
@@ -573,7 +691,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int ia = 32 * ch + 8 * t + 2 * r + i;
-                fxy[i] = ia < P.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, iy, gz)) * face_k : 0.0;
+                fxy[i] = ia < Q.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, iy, gz)) * face_k : 0.0;
               }
             }
 
@@ -611,7 +729,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
 
         // ---- accumulate vo in the region's visiting order
         if (gvo) {
-          double* vdst = P.vo + col + slab * (size_t)g_vo + (size_t)(slab * P.ne) * (size_t)iz + (vo_lane - (r >> 1) * (VSZ / 2));
+          double* vdst = Q.vo + col + slab * (size_t)g_vo + (size_t)(slab * Q.ne) * (size_t)iz + (vo_lane - (r >> 1) * (VSZ / 2));
           const double* vold = stg + C::ST_VO + warp * VSZ + vo_lane;
 #pragma unroll
           for (int mt = 0; mt < MT; ++mt)
@@ -635,6 +753,102 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const
     if (stop) break;
   }
   cp_async_wait<0>();  // no copy into shared memory outlives the CTA
+  }
+}
+
+template <int NM_, int NCH, int TX, int TY, int NS, bool PIPE_T1>
+__global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_kernel(const Fp64Params P) {
+  fp64_body<NM_, NCH, TX, TY, NS, PIPE_T1, false, 0>(P, 0);
+}
+
+// Batched FP64 sweep: one class kind per (NM, angle chunks, tile shape), all
+// with 8 compute warps + the producer warpgroup (384 threads).  The CTAs work
+// through the classes in order; a CTA moves on when its class's table is
+// exhausted, so a task only ever waits on tasks that CTAs hold and advance.
+enum Fp64BatchKind {
+  BK_NM4_C1_42 = 0, BK_NM4_C1_24, BK_NM4_C2_42, BK_NM4_C2_24,
+  BK_NM8_C1_42, BK_NM8_C1_24, BK_NM8_C2_42, BK_NM8_C2_24,
+  BK_NM16_C1_42, BK_NM16_C1_24, BK_NM16_C2_42, BK_NM16_C2_24,
+  BK_COUNT
+};
+constexpr int batch_kind(int nm, int nch, bool tile24) {
+  return (nm == 4 ? 0 : nm == 8 ? 4 : 8) + (nch == 2 ? 2 : 0) + (tile24 ? 1 : 0);
+}
+
+// Every body kind of the batched kernel, in increasing kind order:
+// F(kind, NM, NCH, TX, TY).
+#define MSB_FP64_BATCH_KINDS(F)                                                                   \
+  F(BK_NM4_C1_42, 4, 1, 4, 2) F(BK_NM4_C1_24, 4, 1, 2, 4) F(BK_NM4_C2_42, 4, 2, 4, 2)             \
+  F(BK_NM4_C2_24, 4, 2, 2, 4) F(BK_NM8_C1_42, 8, 1, 4, 2) F(BK_NM8_C1_24, 8, 1, 2, 4)             \
+  F(BK_NM8_C2_42, 8, 2, 4, 2) F(BK_NM8_C2_24, 8, 2, 2, 4) F(BK_NM16_C1_42, 16, 1, 4, 2)           \
+  F(BK_NM16_C1_24, 16, 1, 2, 4) F(BK_NM16_C2_42, 16, 2, 4, 2) F(BK_NM16_C2_24, 16, 2, 2, 4)
+
+// Between two classes: every warp of the CTA is done with the previous
+// class's stages (a barrier that warps reach from their own role's code, so
+// the non-aligned form), thread 0 swaps the barrier sets, and nobody starts
+// the new class before that.
+template <int NS>
+__device__ __forceinline__ void fp64_batch_switch(const Fp64Batch& P, int c) {
+  asm volatile("barrier.sync 0;" ::: "memory");
+  if (threadIdx.x == 0) {
+#define MSB_K(K, NM, NCH, TX, TY) \
+  case K: fp64_barriers<NM, NCH, TX, TY, NS>(init); break;
+    for (int k = 0; k < 2; ++k) {
+      const bool init = k == 1;
+      const int cc = init ? c : c - 1;
+      if (cc < 0 || cc >= P.nclass) continue;
+      switch (P.cls_kind[cc]) { MSB_FP64_BATCH_KINDS(MSB_K) default: break; }
+    }
+#undef MSB_K
+  }
+  asm volatile("barrier.sync 0;" ::: "memory");
+}
+
+// The classes of a launch come in increasing kind order (the host sorts
+// them so), and the kernel visits the kinds in that order, one straight-line
+// region per kind: compiled as separate regions (rather than the cases of a
+// switch) the bodies keep their register allocations apart.
+template <int NS>
+__global__ void __launch_bounds__(12 * 32, 1) sweep_fp64_batch_kernel(const Fp64Batch P) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) P.ptime[P.nprob] = global_ns();
+  // the register split of the 8-compute-warp bodies, once for all classes
+  if ((threadIdx.x >> 5) >= 8) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Fp64Cfg<16, 1, 4, 2, NS>::REG_PRODUCER));
+    int c = 0;
+#define MSB_K(K, NM, NCH, TX, TY)                                 \
+  if (c < P.nclass && P.cls_kind[c] == K) {                       \
+    fp64_batch_switch<NS>(P, c);                                  \
+    fp64_body<NM, NCH, TX, TY, NS, false, true, 1>(P, c);         \
+    ++c;                                                          \
+  }
+    MSB_FP64_BATCH_KINDS(MSB_K)
+#undef MSB_K
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Fp64Cfg<16, 1, 4, 2, NS>::REG_COMPUTE));
+    int c = 0;
+#define MSB_K(K, NM, NCH, TX, TY)                                 \
+  if (c < P.nclass && P.cls_kind[c] == K) {                       \
+    fp64_batch_switch<NS>(P, c);                                  \
+    fp64_body<NM, NCH, TX, TY, NS, false, true, 2>(P, c);         \
+    ++c;                                                          \
+  }
+    MSB_FP64_BATCH_KINDS(MSB_K)
+#undef MSB_K
+  }
+}
+
+// Dynamic shared memory of the batched kernel: the largest class body.
+template <int NS>
+constexpr size_t fp64_batch_smem() {
+  size_t m = 0;
+  const size_t v[] = {Fp64Cfg<4, 1, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<4, 1, 2, 4, NS>::smem_bytes_batch(),
+                      Fp64Cfg<4, 2, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<4, 2, 2, 4, NS>::smem_bytes_batch(),
+                      Fp64Cfg<8, 1, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<8, 1, 2, 4, NS>::smem_bytes_batch(),
+                      Fp64Cfg<8, 2, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<8, 2, 2, 4, NS>::smem_bytes_batch(),
+                      Fp64Cfg<16, 1, 4, 2, NS>::smem_bytes_batch(), Fp64Cfg<16, 1, 2, 4, NS>::smem_bytes_batch(),
+                      Fp64Cfg<16, 2, 4, 2, NS>::smem_bytes_batch(), Fp64Cfg<16, 2, 2, 4, NS>::smem_bytes_batch()};
+  for (size_t x : v) m = x > m ? x : m;
+  return m;
 }
 
 }  // namespace msb

@@ -275,33 +275,34 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
       return rc;
   }
   if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
-  auto fill = [&](auto& P, auto* face) {
+  // problem fields (X) and schedule fields (P)
+  auto fill = [&](auto& X, auto& P, auto* face) {
     using F = std::remove_pointer_t<decltype(face)>;
-    P.vi = vi_d;
-    P.afm = S.d_afm;
-    P.mfa = S.d_mfa;
-    P.fxy = static_cast<F*>(S.d_face[0]);
-    P.fxz = static_cast<F*>(S.d_face[1]);
-    P.fyz = static_cast<F*>(S.d_face[2]);
+    X.vi = vi_d;
+    X.afm = S.d_afm;
+    X.mfa = S.d_mfa;
+    X.fxy = static_cast<F*>(S.d_face[0]);
+    X.fxz = static_cast<F*>(S.d_face[1]);
+    X.fyz = static_cast<F*>(S.d_face[2]);
+    X.nx = S.dims.ncell_x;
+    X.ny = S.dims.ncell_y;
+    X.nz = S.dims.ncell_z;
+    X.ne = S.dims.ne;
+    X.na = S.dims.na;
+    X.ngp = S.ngp;
     P.tasks = S.d_tasks;
     P.ntask = S.sched.ntask();
-    P.nx = S.dims.ncell_x;
-    P.ny = S.dims.ncell_y;
-    P.nz = S.dims.ncell_z;
-    P.ne = S.dims.ne;
-    P.na = S.dims.na;
-    P.ngp = S.ngp;
     P.sy.sync = S.d_sync;
     P.sy.timeout_ns = S.timeout_ns;
   };
   if (S.var.fn) {
     Fp64Params P;
-    fill(P, (double*)nullptr);
-    P.vo = vo_d;
+    fill(P.pr, P, (double*)nullptr);
+    P.pr.vo = vo_d;
     S.var.fn<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
   } else {
     MixParams P;
-    fill(P, (float*)nullptr);
+    fill(P, P, (float*)nullptr);
     P.part = S.d_part;
     P.state = S.part_elems / NOCTANT;
     if ((rc = encode_state_map(&P.tm_vi, vi_d, S.dims, &P.vbox_bytes))) return rc;
