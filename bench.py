@@ -307,6 +307,69 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
     return out
 
 
+def measure_dense(args, dev, world: int, local_rank: int) -> dict | None:
+    """The angle/group-heavy case: 32x32x96 cells, ne 128, na 128, NM 16,
+    nblock_z 12, built-in Quantities.  One FP64 sweep (two 64-angle passes,
+    tile shape autotuned by the untimed first sweep) against one sweep of each
+    mixed precision (four 32-angle passes), each timed after one untimed
+    sweep; under torchrun each rank sweeps its own 128-group slice.  The FP64
+    sweep of the built-in problem returns its input exactly, so the mixed
+    errors are measured against the initial state."""
+    if args.no_dense:
+        return None
+    import torch
+
+    import minisweep_b200 as msb
+    from minisweep_b200.parallel import max_over_ranks
+
+    nx, ny, nz, ne, na, nm, nbz = 32, 32, 96, 128, 128, 16, 12
+    fl = f"--ncell_x {nx} --ncell_y {ny} --ncell_z {nz} --ne {ne} --na {na} --nblock_z {nbz}"
+    upd = nx * ny * nz * ne * na * 8
+    flops = flops_per_sweep(nx, ny, nz, ne, na, nm)
+    out = {"workload": f"{nx}x{ny}x{nz} cells, ne {ne}, na {na}, NM {nm}, NU {NU}, nblock_z {nbz}, built-in "
+                       f"Quantities, one sweep per timing (after one untimed sweep)",
+           "updates_per_sweep": upd, "flops_per_sweep": flops, "runs": []}
+    va = vb = None
+    clocks = Clocks(local_rank)
+    clocks.start()
+    for prec in (0, 1, 2):
+        with msb.Problem(fl + (" --autotune 1" if prec == 0 else f" --precision {prec}"), nm=nm) as pb:
+            if va is None:
+                va = torch.empty(pb.nstate, dtype=torch.float64, device=dev)
+                vb = torch.empty_like(va)
+            pb.init_state_device(va.data_ptr())
+            torch.cuda.synchronize()
+            st = torch.cuda.ExternalStream(pb.stream) if pb.stream else torch.cuda.current_stream()
+            pb.sweep_device(vb.data_ptr(), va.data_ptr())
+            pb.sync()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            pb.sweep_device(vb.data_ptr(), va.data_ptr())
+            e1.record(st)
+            pb.sync()
+            torch.cuda.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1) / 1e3) * 1e3
+            r = {"precision": prec, "ms_per_sweep": ms, "updates_per_s": upd * world / (ms * 1e-3),
+                 "launches_per_sweep": (na + 63) // 64 if prec == 0 else 2 * ((na + 31) // 32)}
+            if prec == 0:
+                r["exact"] = bool(torch.equal(va, vb))
+                r["tflops"] = flops / (ms * 1e-3) / 1e12
+                r["tile"] = pb.tile()
+            else:
+                r["max_rel"] = (torch.max(torch.abs(vb - va)) / torch.max(torch.abs(va))).item()
+                nf = torch.sum(va * va)
+                r["normsq_rel"] = abs((torch.sum(vb * vb) - nf) / nf).item()
+            out["runs"].append(r)
+    out["clocks"] = clocks.stop()
+    f64 = out["runs"][0]["ms_per_sweep"]
+    for r in out["runs"][1:]:
+        r["speedup_vs_fp64"] = f64 / r["ms_per_sweep"]
+    del va, vb
+    torch.cuda.empty_cache()
+    return out
+
+
 def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict | None:
     """The batched serving workload: 256 independent problems (seed 7, sizes in
     msb.batch_workload), every one swept by ONE persistent launch per sweep;
@@ -438,7 +501,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
 
     flags = (f"--ncell_x {NX} --ncell_y {NY} --ncell_z {NZ} --ne {NE} --na {NA} --nblock_z {NBLOCK_Z} "
              f"--niterations {NITER}")
-    pb = msb.Problem(flags, nm=NM)
+    # --autotune 1: the first (warm-up) sweep times both FP64 tile shapes and
+    # keeps the faster for every later sweep
+    pb = msb.Problem(flags + " --autotune 1", nm=NM)
     n = pb.nstate
     va = torch.empty(n, dtype=torch.float64, device=dev)
     vb = torch.empty(n, dtype=torch.float64, device=dev)
@@ -464,6 +529,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     for _ in range(args.warmup):
         one_step()
     pb.sync()
+    tile = pb.tile()
     barrier()
     clocks = Clocks(local_rank)
     clocks.start()
@@ -495,6 +561,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     def finish(e2e):
         pb.close()
         batched = measure_batched(args, dev, world, rank, local_rank)
+        dense = measure_dense(args, dev, world, local_rank)
         upd = updates_per_sweep() * NITER
         value = upd * args.steps * world / elapsed
         ms_sweep = sum(sweep_ms) / len(sweep_ms)
@@ -529,7 +596,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                     "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                     "data": "synthetic: the reference's built-in deterministic Quantities (index-derived state, "
                             "faces and transform matrices)",
-                    "config": dict(config_dict(), parallelism=f"{world} GPU(s) x 64-group slice, no exchange"),
+                    "config": dict(config_dict(), parallelism=f"{world} GPU(s) x 64-group slice, no exchange",
+                                   tile={"cells_per_cta": [tile["tx"], tile["ty"]],
+                                         "autotune_first_sweep_ms": {"chosen": tile["ms_chosen"],
+                                                                     "other": tile["ms_other"]}}),
                     "roofline": roofline, "cpu_baseline": cpu,
                     "e2e": e2e,
                     "clocks": clk, "gpu_launches": args.steps * NITER,
@@ -539,7 +609,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                     "check": {"normsq": normsq, "normsqdiff": normsqdiff, "normsq_closed_form": closed,
                               "pass": normsqdiff == 0.0 and (closed is None or normsq == closed)},
                     "ms_per_sweep_kernel": ms_sweep,
-                    "batched": batched}
+                    "batched": batched,
+                    "dense_case": dense}
             print(json.dumps(line), flush=True)
         if dist is not None:
             dist.destroy_process_group()
@@ -581,6 +652,7 @@ def main() -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched serving workload")
+    ap.add_argument("--no-dense", action="store_true", help="skip the 32x32x96 / ne 128 / na 128 case")
     ap.add_argument("--batch-steps", type=int, default=2, help="timed batched sweeps")
     ap.add_argument("--batch-warmup", type=int, default=1, help="untimed batched sweeps")
     ap.add_argument("--case", choices=["config2", "small"], default="config2",
@@ -593,6 +665,7 @@ def main() -> int:
         args.no_cpu = True
         args.no_e2e = True
         args.no_batch = True
+        args.no_dense = True
         WORKLOAD = WORKLOAD.replace("64x64x64", "32x32x32").replace("ne 64", "ne 32").replace(
             "niterations 10", "niterations 1")
     else:

@@ -332,6 +332,11 @@ int msb_state_norms_device(const double* vi_d, const double* vo_d, size_t n,
 int msb_initialize_state_device(double* v_d, Dimensions dims, Env* env);
 /* Kernel statistics of the last sweep: number of tasks, kernel launches. */
 int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int* nlaunch);
+/* Tile shape (cell columns per CTA) the sweeper uses and, with --autotune 1,
+ * the first sweep's times (ms) of the chosen and the other shape (0 before
+ * that sweep, or without autotuning).  No reference counterpart: the
+ * reference's --ncell_{x,y}_per_subblock size its CPU/GPU thread blocks. */
+int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_chosen, float* ms_other);
 /* Copy of the schedule (one record of MSB_TASK_INTS ints per task, in launch
  * order) for host-side checks; returns the task count, or <0. */
 enum { MSB_TASK_INTS = 16 };

@@ -117,6 +117,8 @@ def lib() -> ctypes.CDLL:
         L.Sweeper_debug_tasks.argtypes = [P(Sweeper), P(ctypes.c_int), ctypes.c_longlong]
         L.Sweeper_debug_tasks.restype = ctypes.c_longlong
         L.Sweeper_set_spin_limit.argtypes = [P(Sweeper), ctypes.c_longlong]
+        L.Sweeper_tile.argtypes = [P(Sweeper), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_float),
+                                   P(ctypes.c_float)]
         L.msb_state_norms_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, P(D), P(D), P(Env)]
         L.msb_initialize_state_device.argtypes = [ctypes.c_void_p, Dimensions, P(Env)]
         L.msb_schedule_tasks.argtypes = [ctypes.c_int] * 7 + [P(ctypes.c_int), ctypes.c_longlong]
@@ -288,6 +290,15 @@ class Problem:
         L.Sweeper_debug_tasks(ctypes.byref(self.sweeper), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
         return out
 
+    def tile(self) -> dict:
+        """Tile shape in use and, with --autotune 1, the first sweep's times of
+        the chosen and the other shape (ms)."""
+        tx, ty = ctypes.c_int(), ctypes.c_int()
+        a, b = ctypes.c_float(), ctypes.c_float()
+        _check(lib().Sweeper_tile(ctypes.byref(self.sweeper), ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(a),
+                                  ctypes.byref(b)))
+        return {"tx": tx.value, "ty": ty.value, "ms_chosen": a.value, "ms_other": b.value}
+
     def set_timeout_ns(self, ns: int) -> None:
         _check(lib().Sweeper_set_spin_limit(ctypes.byref(self.sweeper), ns))
 
@@ -420,6 +431,15 @@ class Batch:
         pred = np.zeros(max(npred, 1), dtype=np.int32)
         _check(min(0, L.msb_batch_scratch(self._h, None, None, None, pred.ctypes.data_as(IP), len(pred))))
         return off, nb, po, pred[:npred]
+
+    def tile(self) -> dict:
+        """Tile shape in use and, with --autotune 1, the first sweep's times of
+        the chosen and the other shape (ms)."""
+        tx, ty = ctypes.c_int(), ctypes.c_int()
+        a, b = ctypes.c_float(), ctypes.c_float()
+        _check(lib().Sweeper_tile(ctypes.byref(self.sweeper), ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(a),
+                                  ctypes.byref(b)))
+        return {"tx": tx.value, "ty": ty.value, "ms_chosen": a.value, "ms_other": b.value}
 
     def set_timeout_ns(self, ns: int) -> None:
         _check(lib().msb_batch_set_spin_limit(self._h, ns))

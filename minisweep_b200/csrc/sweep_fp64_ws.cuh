@@ -58,6 +58,8 @@ struct Fp64Prob {
   double* fxz;
   double* fyz;
   int nx, ny, nz, ne, na, ngp;
+  int ia_base;  // angle index of the first angle of afm / mfa (a multiple of 64: passes over na > 64)
+  int vo_add;   // nonzero: every phase adds to vo (the passes after the first)
 };
 
 // One problem per launch.
@@ -511,7 +513,7 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
     const size_t slab = (size_t)NM_ * NU * Q.nx * Q.ny;  // one (iz, ie) layer of the state
     const int w = x1 - x0, h = y1 - y0, nzr = z1 - z0, nsteps = nzr + w + h - 2;
     const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
-    const bool first = (flags & TF_FIRST) != 0;
+    const bool first = (flags & TF_FIRST) != 0 && !Q.vo_add;
     const bool act = wa < w && wb < h;
     const int ix = dx > 0 ? x0 + wa : x1 - 1 - wa;
     const int iy = dy > 0 ? y0 + wb : y1 - 1 - wb;
@@ -662,8 +664,8 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
             } else {
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
-                const int ia = 32 * ch + 8 * t + 2 * r + i;
-                fyz[i] = ia < Q.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(gx, iy, iz)) * face_k : 0.0;
+                const int ia = 32 * ch + 8 * t + 2 * r + i, iag = Q.ia_base + ia;
+                fyz[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(gx, iy, iz)) * face_k : 0.0;
               }
             }
             if (in_xz) {
@@ -675,8 +677,8 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
             } else {
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
-                const int ia = 32 * ch + 8 * t + 2 * r + i;
-                fxz[i] = ia < Q.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, gy, iz)) * face_k : 0.0;
+                const int ia = 32 * ch + 8 * t + 2 * r + i, iag = Q.ia_base + ia;
+                fxz[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(ix, gy, iz)) * face_k : 0.0;
               }
             }
             if (c > 0) {
@@ -690,8 +692,8 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
             } else {
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
-                const int ia = 32 * ch + 8 * t + 2 * r + i;
-                fxy[i] = ia < Q.na ? (double)((1 + ia) << (ia & 7)) * d_pow2(d_log2_space(ix, iy, gz)) * face_k : 0.0;
+                const int ia = 32 * ch + 8 * t + 2 * r + i, iag = Q.ia_base + ia;
+                fxy[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(ix, iy, gz)) * face_k : 0.0;
               }
             }
 

@@ -44,12 +44,13 @@
 // face from lane l-8 of its own tile row and its xz face from tile row b-1;
 // the xy face is the thread's own register copy (`carry`).
 //
-// Pipelining per global step G (TMEM accumulators indexed by G % 2):
-//   wait T1(G); half 0: convert vi(G+1) -> A1, barrier of half 0, T1(G+1) issued
-//   read D1(G), solve, faces out; wait T2(G-1); half 1: vo += D2(G-1);
-//   write A2(G); barrier of all compute warps; T2(G) issued
-// so T1 has most of a step and T2 a whole solve to finish before they are
-// read, and the vo update trails the solve by one step.
+// Pipelining per global step G (TMEM accumulators and A2 indexed by G % 2):
+//   wait T1(G); read D1(G); convert vi(G+1) -> A1, barrier, T1(G+1) issued;
+//   solve, write A2(G), faces out; wait T2(G-1), vo partial += D2(G-1);
+//   barrier of all compute warps; T2(G) issued; stage G handed back
+// so T1 has most of a step and T2 a whole step to finish before they are
+// read, the vo update trails the solve by one step, and no step waits for
+// the previous step's T2 before writing its own A2.
 #pragma once
 
 #include <cuda.h>
@@ -79,6 +80,7 @@ struct MixParams {
   const int* tasks;
   long long ntask;
   int nx, ny, nz, ne, na, ngp;
+  int ia_base;     // angle index of the first angle of afm / mfa (32-angle passes over a larger na)
   int vbox_bytes;  // bytes one TMA box delivers (both groups; one group when ne == 1)
   SyncArgs sy;
 };
@@ -225,8 +227,8 @@ struct MixCfg {
   // shared-memory layout (bytes)
   static constexpr int SM_STAGE = 0;
   static constexpr int SM_A1 = SM_STAGE + NS * STAGE;  // [hi, lo]
-  static constexpr int SM_A2 = SM_A1 + 2 * A1M;       // [hi, lo]
-  static constexpr int SM_MAT = SM_A2 + 2 * A2M;      // [2 buffers][B1 hi, B1 lo, B2 hi, B2 lo]
+  static constexpr int SM_A2 = SM_A1 + 2 * A1M;       // [step parity][hi, lo]
+  static constexpr int SM_MAT = SM_A2 + 4 * A2M;      // [2 buffers][B1 hi, B1 lo, B2 hi, B2 lo]
   static constexpr int SM_SLOT = SM_MAT + 2 * MATBUF;  // [2 parity][tile row][2 halves]
   static constexpr int SM_KS = SM_SLOT + 2 * TY * 2 * SLOT;  // row scales k1, k2: [2][2][128] ints
   static constexpr int SM_BAR = SM_KS + 2 * 2 * 2 * 128 * 4;
@@ -576,10 +578,12 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       if (lane == 0) {
 #pragma unroll
         for (int kk = 0; kk < 2; ++kk) {
-          const uint32_t o = 256u * kk, d = tmem + C::TM_D2 + (uint32_t)(gg & 1) * 32 + 16u * kk;
-          umma_f16(d, umma_sdesc(a2u + C::A2M + o, 128, 512), umma_sdesc(b2 + o, 128, 512), ID2, 0);
-          umma_f16(d, umma_sdesc(a2u + o, 128, 512), umma_sdesc(b2 + C::B2M + o, 128, 512), ID2, 1);
-          umma_f16(d, umma_sdesc(a2u + o, 128, 512), umma_sdesc(b2 + o, 128, 512), ID2, 1);
+          // o: this angle half's K chunk in A2 and B2; A2 also by step parity
+          const uint32_t o = 256u * kk, a2 = a2u + (uint32_t)(gg & 1) * 2 * C::A2M + o;
+          const uint32_t d = tmem + C::TM_D2 + (uint32_t)(gg & 1) * 32 + 16u * kk;
+          umma_f16(d, umma_sdesc(a2 + C::A2M, 128, 512), umma_sdesc(b2 + o, 128, 512), ID2, 0);
+          umma_f16(d, umma_sdesc(a2, 128, 512), umma_sdesc(b2 + C::B2M + o, 128, 512), ID2, 1);
+          umma_f16(d, umma_sdesc(a2, 128, 512), umma_sdesc(b2 + o, 128, 512), ID2, 1);
         }
         umma_commit(&d2bar[gg & 1]);
       }
@@ -606,11 +610,14 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         bar_step();  // end of step G
         if (s_abort) { quit = true; break; }
         issue_t2(G, b2u);
-        if (s > 0 && lane == 0) mbar_arrive(&done[(G - 1) % NS]);  // vo of step G - 1 written
+        // step G's stage is consumed and its faces are written: the
+        // publisher may publish its progress and hand the stage back (the vo
+        // partials need no ordering: each octant writes its own array, read
+        // only by the next kernel)
+        if (lane == 0) mbar_arrive(&done[G % NS]);
         if (s == nsteps - 1) {
           bar_step();  // the task's last vo written
           if (s_abort) { quit = true; break; }
-          if (lane == 0) mbar_arrive(&done[G % NS]);
         }
       }
       if (quit) break;
@@ -827,8 +834,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
           auto boundary = [&](float sg, float (&f)[16]) {
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
-              const int ia = ia0 + i;
-              f[i] = ia < P.na ? (float)((1 + ia) << (ia & 7)) * sg * face_k : 0.0f;
+              const int ia = ia0 + i, iag = P.ia_base + ia;
+              f[i] = ia < P.na ? (float)((1 + iag) << (iag & 7)) * sg * face_k : 0.0f;
             }
           };
           if (a > 0) {
@@ -860,8 +867,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         if (act) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
-            const int ia = ia0 + i;
-            const float wz = 0.25f - 1.0f / (float)(1 << (ia & 7));
+            const int iag = P.ia_base + ia0 + i;
+            const float wz = 0.25f - 1.0f / (float)(1 << (iag & 7));
             const float sab = __fmaf_rn(fxy[i], cxy, __fmul_rn(fxz[i], cxz));
             const float sm = __fmaf_rn(fyz[i], __fmul_rn(wz, sx_r), sab);
             float vs = __fmul_rn(__fmul_rn(v[i], vsc1), vsc2);
@@ -872,9 +879,10 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             carry[i] = __fmul_rn(psi, so);
           }
         }
-        // ---- the previous step's T2 is done: A2 is free, D2 readable
-        if (has_pend) wait(&d2bar[pend.gg & 1], pend.gg, 2);
-        // ---- psi (this half's 16 angles) -> scaled hi/lo, K-chunks 2*half, 2*half+1 of A2
+        // ---- psi (this half's 16 angles) -> scaled hi/lo, K-chunks 2*half,
+        // 2*half+1 of A2 buffer G % 2, last read by T2(G - 2), whose completion
+        // this thread saw before the vo update of step G - 2 (one step ago)
+        unsigned char* const a2b = a2s + (size_t)(G & 1) * 2 * C::A2M;
         int k2 = 0;
         if (act) {
           k2 = split_scale_f(pmax);
@@ -890,8 +898,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
               lo[p] = H::pack(__fsub_rn(x0, hv.x), __fsub_rn(x1, hv.y));
             }
             const int off = kmajor_off(row, 16 * half + 8 * kc, 128, 512);
-            *reinterpret_cast<uint4*>(a2s + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4*>(a2s + C::A2M + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            *reinterpret_cast<uint4*>(a2b + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4*>(a2b + C::A2M + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
           }
         }
         k2s[(G & 1) * 256 + half * 128 + row] = k2;
@@ -909,7 +917,10 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
           }
         }
         // ---- vo of the previous step (its products had this step to finish)
-        if (has_pend) epilogue(pend);
+        if (has_pend) {
+          wait(&d2bar[pend.gg & 1], pend.gg, 2);
+          epilogue(pend);
+        }
         pend = Pend{G, act ? part_oct + (size_t)((long long)row0 + zstep * c) : nullptr, k2, act};
         has_pend = true;
         // ---- step barrier: A2 rows, slots and row scales of step G complete
@@ -939,13 +950,23 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
 }
 
 // vo = sum over the eight octants of their FP32 partials, in FP64 and in
-// octant order (deterministic).  n is a multiple of 4 (NM * NU elements per
-// (cell, group)).
+// octant order (deterministic); with `accumulate` the sum is added to vo (the
+// angle passes after the first of a larger na).  n is a multiple of 4
+// (NM * NU elements per (cell, group)).
 __global__ void __launch_bounds__(256) reduce_octant_partials(double* __restrict__ vo,
-                                                              const float* __restrict__ part, size_t n) {
+                                                              const float* __restrict__ part, size_t n,
+                                                              int accumulate) {
   const size_t n4 = n / 4;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (accumulate) {
+      const double2* d = reinterpret_cast<const double2*>(vo) + 2 * i;
+      const double2 p0 = __ldcs(d), p1 = __ldcs(d + 1);
+      a0 = p0.x;
+      a1 = p0.y;
+      a2 = p1.x;
+      a3 = p1.y;
+    }
 #pragma unroll
     for (int o = 0; o < NOCTANT; ++o) {
       const float4 q = __ldcs(reinterpret_cast<const float4*>(part + n * o) + i);

@@ -57,13 +57,15 @@ Variant make_variant() {
   return v;
 }
 
+// FP64 tile shapes: 4 x 2 (tile 42, the default) or 2 x 4 (tile 24) cell
+// columns, for one or two 32-angle chunks per pass (na > 64 is swept in
+// passes of 64 angles).
 template <int NM_>
-Variant pick_nch(int nch) {
+Variant pick_nch(int nch, int tile) {
+  const bool t24 = tile == 24;
   switch (nch) {
-    case 1: return make_variant<NM_, 1, 4, 2>();
-    case 2: return make_variant<NM_, 2, 4, 2>();
-    case 3:
-    case 4: return make_variant<NM_, 4, 2, 2>();
+    case 1: return t24 ? make_variant<NM_, 1, 2, 4>() : make_variant<NM_, 1, 4, 2>();
+    case 2: return t24 ? make_variant<NM_, 2, 2, 4>() : make_variant<NM_, 2, 4, 2>();
     default: return Variant();
   }
 }
@@ -95,19 +97,21 @@ Variant pick_mixed(int nm) {
   }
 }
 
-// precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves
-// (the mixed kernels take na <= 32).
-Variant pick_variant(int nm, int na, int precision) {
+// precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves.
+// tile: 0 = the default shape, 42 or 24 (FP64 only).  na <= 128: the FP64
+// kernels sweep 64 angles per pass, the mixed ones 32.
+Variant pick_variant(int nm, int na, int precision, int tile = 0) {
+  if (na > 128) return Variant();
   if (precision == 1 || precision == 2) {
-    if (na > 32) return Variant();
+    if (tile != 0) return Variant();
     return precision == 1 ? pick_mixed<MIX_F16>(nm) : pick_mixed<MIX_BF16>(nm);
   }
   if (precision != 0) return Variant();
-  const int nch = (na + 31) / 32;
+  const int nch = na > 32 ? 2 : 1;
   switch (nm) {
-    case 4: return pick_nch<4>(nch);
-    case 8: return pick_nch<8>(nch);
-    case 16: return pick_nch<16>(nch);
+    case 4: return pick_nch<4>(nch, tile);
+    case 8: return pick_nch<8>(nch, tile);
+    case 16: return pick_nch<16>(nch, tile);
     default: return Variant();
   }
 }
@@ -159,6 +163,15 @@ int encode_state_map(CUtensorMap* map, const double* ptr, const Dimensions& d, i
 
 }  // namespace
 
+// The other FP64 tile shape of an autotuning sweeper, with its own schedule.
+struct AltPlan {
+  Variant var;
+  Schedule sched;
+  int gp_block = 1;
+  int* d_tasks = nullptr;
+  int grid = 0;
+};
+
 struct SweeperImpl {
   Dimensions dims{};
   int precision = 0;
@@ -176,51 +189,93 @@ struct SweeperImpl {
   double* d_mfa = nullptr;
   float* d_part = nullptr;  // mixed precision: FP32 partial vo per octant
   size_t part_elems = 0;
+  double* d_afm_c = nullptr;  // na above one pass: the pass's angle range of each matrix
+  double* d_mfa_c = nullptr;
   double* d_vi = nullptr;  // staging for host-only Pointers
   double* d_vo = nullptr;
   long long timeout_ns = kDefaultTimeoutNs;
   int nlaunch = 0;
   int nsm = 0;
   int* h_status = nullptr;  // pinned copy of the status words
+  // --autotune 1: the first sweep runs with both tile shapes and keeps the faster
+  bool autotune = false;
+  bool tuned = false;
+  AltPlan alt;
+  float tune_ms[2] = {0.f, 0.f};  // first sweep: the chosen shape, the other shape
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
+    cudaFree(alt.d_tasks);
     cudaFree(d_sync);
     for (auto& f : d_face) cudaFree(f);
     cudaFree(d_afm);
     cudaFree(d_mfa);
     cudaFree(d_part);
+    cudaFree(d_afm_c);
+    cudaFree(d_mfa_c);
     cudaFree(d_vi);
     cudaFree(d_vo);
     if (h_status) cudaFreeHost(h_status);
   }
 };
 
-static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision) {
+// Angles per pass: the FP64 kernels sweep up to 64 (two 32-angle chunks) at
+// once, the mixed ones 32.  Angles are independent in the sweep (each has its
+// own faces), so a larger na is swept in passes over consecutive angle
+// ranges whose contributions add up in vo.
+static int pass_angles(const SweeperImpl& S) { return S.var.mix ? 32 : 64; }
+
+// Schedule, device task table and grid of one compiled tile shape.
+static int setup_plan(const SweeperImpl& S, const Variant& var, Schedule& sched, int& gp_block, int*& d_tasks,
+                      int& grid) {
+  const Dimensions& dims = S.dims;
+  int rc, occ = 0;
+  gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, var.tx, var.ty, 2 * S.nsm);
+  if ((rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, var.tx, var.ty, gp_block, sched)))
+    return rc;
+  const long long ntask = sched.ntask();
+  if (ntask >= (1LL << 31) - SY_PROGRESS) return set_error(MSB_ERR_ARG, "too many tasks");
+  if ((rc = cuda_check(cudaMalloc(&d_tasks, sched.rec.size() * sizeof(int)), "cudaMalloc tasks"))) return rc;
+  if ((rc = cuda_check(cudaMemcpy(d_tasks, sched.rec.data(), sched.rec.size() * sizeof(int), cudaMemcpyHostToDevice),
+                       "copy tasks")))
+    return rc;
+  if ((rc = cuda_check(cudaFuncSetAttribute(var.func(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)var.smem),
+                       "cudaFuncSetAttribute")))
+    return rc;
+  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, var.func(), var.threads, var.smem),
+                       "occupancy")))
+    return rc;
+  if (occ < 1) return set_error(MSB_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
+  grid = (int)std::min<long long>(ntask, (long long)S.nsm * occ);
+  return MSB_OK;
+}
+
+static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, int tile = 0, bool autotune = false) {
   S.dims = dims;
   S.precision = precision;
   if (dims.ncell_x <= 0 || dims.ncell_y <= 0 || dims.ncell_z <= 0 || dims.ne <= 0 || dims.na <= 0)
     return set_error(MSB_ERR_ARG, "invalid dimensions");
-  S.var = pick_variant(dims.nm, dims.na, precision);
+  S.var = pick_variant(dims.nm, dims.na, precision, tile);
   if (!S.var.valid())
     return set_error(MSB_ERR_UNSUPPORTED,
-                     "no kernel variant for nm=%d na=%d precision=%d (nm in {4,8,16}; na <= 128 for FP64, "
-                     "na <= 32 for the mixed kernels)",
-                     dims.nm, dims.na, precision);
+                     "no kernel variant for nm=%d na=%d precision=%d tile=%d (nm in {4,8,16}; na <= 128; "
+                     "--tile 42 / 24 only for the FP64 sweep)",
+                     dims.nm, dims.na, precision, tile);
+  if (autotune && precision != 0)
+    return set_error(MSB_ERR_UNSUPPORTED, "--autotune 1 needs the FP64 sweep (the mixed sweep has one tile shape)");
   S.ngp = (dims.ne + 1) / 2;
-  int rc, dev = 0, nsm = 0, occ = 0;
+  int rc, dev = 0, nsm = 0;
   if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
   if ((rc = cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rc;
-  S.gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, S.var.tx, S.var.ty, 2 * nsm);
-  rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, S.var.tx, S.var.ty, S.gp_block, S.sched);
-  if (rc) return rc;
-  const long long ntask = S.sched.ntask();
-  if (ntask >= (1LL << 31) - SY_PROGRESS) return set_error(MSB_ERR_ARG, "too many tasks");
-
-  if ((rc = cuda_check(cudaMalloc(&S.d_tasks, S.sched.rec.size() * sizeof(int)), "cudaMalloc tasks"))) return rc;
-  if ((rc = cuda_check(cudaMemcpy(S.d_tasks, S.sched.rec.data(), S.sched.rec.size() * sizeof(int),
-                                  cudaMemcpyHostToDevice), "copy tasks")))
-    return rc;
+  S.nsm = nsm;
+  if ((rc = setup_plan(S, S.var, S.sched, S.gp_block, S.d_tasks, S.grid))) return rc;
+  long long ntask = S.sched.ntask();
+  if (autotune) {
+    S.autotune = true;
+    S.alt.var = pick_variant(dims.nm, dims.na, precision, S.var.tx == 4 ? 24 : 42);
+    if ((rc = setup_plan(S, S.alt.var, S.alt.sched, S.alt.gp_block, S.alt.d_tasks, S.alt.grid))) return rc;
+    ntask = std::max(ntask, S.alt.sched.ntask());
+  }
   S.sync_ints = SY_PROGRESS + (size_t)ntask;
   if ((rc = cuda_check(cudaMalloc(&S.d_sync, S.sync_ints * sizeof(int)), "cudaMalloc sync"))) return rc;
   if ((rc = cuda_check(cudaMallocHost(&S.h_status, 8 * sizeof(int)), "cudaMallocHost status"))) return rc;
@@ -239,22 +294,115 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision) {
   const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
   if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
   if ((rc = cuda_check(cudaMalloc(&S.d_mfa, nmat * sizeof(double)), "cudaMalloc m_from_a"))) return rc;
-
-  if ((rc = cuda_check(cudaFuncSetAttribute(S.var.func(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)S.var.smem),
-                       "cudaFuncSetAttribute")))
-    return rc;
-  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, S.var.func(), S.var.threads,
-                                                                     S.var.smem),
-                       "occupancy")))
-    return rc;
-  if (occ < 1) return set_error(MSB_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
-  S.grid = (int)std::min<long long>(ntask, (long long)nsm * occ);
-  S.nsm = nsm;
+  if (dims.na > pass_angles(S)) {
+    const size_t npass_mat = (size_t)dims.nm * pass_angles(S) * NOCTANT;
+    if ((rc = cuda_check(cudaMalloc(&S.d_afm_c, npass_mat * sizeof(double)), "cudaMalloc a_from_m pass"))) return rc;
+    if ((rc = cuda_check(cudaMalloc(&S.d_mfa_c, npass_mat * sizeof(double)), "cudaMalloc m_from_a pass"))) return rc;
+  }
   return MSB_OK;
 }
 
-// Launches one sweep: vo_d = sweep(vi_d), asynchronously on `stream`.
+// The columns a0 .. a0 + nac of a_from_m[oct][im][ia] and the rows of
+// m_from_a[oct][ia][im] into the pass buffers (layouts of an na = nac problem).
+static int copy_pass_matrices(SweeperImpl& S, int a0, int nac, cudaStream_t stream) {
+  const int na = S.dims.na, nm = S.dims.nm;
+  int rc = cuda_check(cudaMemcpy2DAsync(S.d_afm_c, nac * sizeof(double), S.d_afm + a0, na * sizeof(double),
+                                        nac * sizeof(double), (size_t)nm * NOCTANT, cudaMemcpyDeviceToDevice, stream),
+                      "a_from_m pass");
+  if (rc) return rc;
+  return cuda_check(cudaMemcpy2DAsync(S.d_mfa_c, (size_t)nac * nm * sizeof(double), S.d_mfa + (size_t)a0 * nm,
+                                      (size_t)na * nm * sizeof(double), (size_t)nac * nm * sizeof(double), NOCTANT,
+                                      cudaMemcpyDeviceToDevice, stream),
+                    "m_from_a pass");
+}
+
+// Before a pass after the first: the task counter and the progress start
+// over; an error (and the abort flag) of an earlier pass stays, so the later
+// passes end at once and the host sees the first error.
+static int reset_pass(SweeperImpl& S, cudaStream_t stream) {
+  int rc = cuda_check(cudaMemsetAsync(S.d_sync + SY_COUNTER, 0, sizeof(int), stream), "reset sync");
+  if (rc) return rc;
+  return cuda_check(cudaMemsetAsync(S.d_sync + SY_PROGRESS, 0, (S.sync_ints - SY_PROGRESS) * sizeof(int), stream),
+                    "reset sync");
+}
+
+// Problem fields (X) and schedule fields (P) of a launch; F is the face type.
+template <class F, class X, class PP>
+static void fill_params(const SweeperImpl& S, X& x, PP& P, const double* vi_d, const int* d_tasks, long long ntask) {
+  x.vi = vi_d;
+  x.afm = S.d_afm;
+  x.mfa = S.d_mfa;
+  x.fxy = static_cast<F*>(S.d_face[0]);
+  x.fxz = static_cast<F*>(S.d_face[1]);
+  x.fyz = static_cast<F*>(S.d_face[2]);
+  x.nx = S.dims.ncell_x;
+  x.ny = S.dims.ncell_y;
+  x.nz = S.dims.ncell_z;
+  x.ne = S.dims.ne;
+  x.na = S.dims.na;
+  x.ngp = S.ngp;
+  x.ia_base = 0;
+  P.tasks = d_tasks;
+  P.ntask = ntask;
+  P.sy.sync = S.d_sync;
+  P.sy.timeout_ns = S.timeout_ns;
+}
+
+// Every pass of one FP64 sweep with the given compiled tile shape.
+static int launch_fp64(SweeperImpl& S, const Variant& var, const int* d_tasks, long long ntask, int grid,
+                       double* vo_d, const double* vi_d, cudaStream_t stream) {
+  const int na = S.dims.na, pa = pass_angles(S), npass = (na + pa - 1) / pa;
+  int rc;
+  for (int c = 0; c < npass; ++c) {
+    Fp64Params P;
+    fill_params<double>(S, P.pr, P, vi_d, d_tasks, ntask);
+    P.pr.vo = vo_d;
+    P.pr.vo_add = c > 0 ? 1 : 0;  // later passes add to vo in every phase
+    if (npass > 1) {
+      const int a0 = pa * c, nac = std::min(pa, na - a0);
+      if ((rc = copy_pass_matrices(S, a0, nac, stream))) return rc;
+      if (c > 0 && (rc = reset_pass(S, stream))) return rc;
+      P.pr.afm = S.d_afm_c;
+      P.pr.mfa = S.d_mfa_c;
+      P.pr.na = nac;
+      P.pr.ia_base = a0;
+    }
+    var.fn<<<grid, var.threads, var.smem, stream>>>(P);
+    if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
+  }
+  return MSB_OK;
+}
+
+// Every pass of one mixed-precision sweep: per pass the sweep kernel writes
+// each octant's FP32 contribution, and the partial sum adds them up in vo.
+static int launch_mixed(SweeperImpl& S, double* vo_d, const double* vi_d, cudaStream_t stream) {
+  const int na = S.dims.na, pa = pass_angles(S), npass = (na + pa - 1) / pa;
+  MixParams P;
+  fill_params<float>(S, P, P, vi_d, S.d_tasks, S.sched.ntask());
+  P.part = S.d_part;
+  P.state = S.part_elems / NOCTANT;
+  int rc;
+  if ((rc = encode_state_map(&P.tm_vi, vi_d, S.dims, &P.vbox_bytes))) return rc;
+  for (int c = 0; c < npass; ++c) {
+    if (npass > 1) {
+      const int a0 = pa * c, nac = std::min(pa, na - a0);
+      if ((rc = copy_pass_matrices(S, a0, nac, stream))) return rc;
+      if (c > 0 && (rc = reset_pass(S, stream))) return rc;
+      P.afm = S.d_afm_c;
+      P.mfa = S.d_mfa_c;
+      P.na = nac;
+      P.ia_base = a0;
+    }
+    S.var.mix<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
+    if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
+    reduce_octant_partials<<<S.nsm * 8, 256, 0, stream>>>(vo_d, S.d_part, P.state, c > 0 ? 1 : 0);
+    if ((rc = cuda_check(cudaGetLastError(), "partial sum launch"))) return rc;
+  }
+  return MSB_OK;
+}
+
+// Launches one sweep: vo_d = sweep(vi_d), asynchronously on `stream` (the
+// first sweep of an autotuning sweeper waits for the stream).
 static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
                       const double* afm_d, const double* mfa_d, cudaStream_t stream) {
   int rc;
@@ -275,46 +423,50 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
       return rc;
   }
   if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
-  // problem fields (X) and schedule fields (P)
-  auto fill = [&](auto& X, auto& P, auto* face) {
-    using F = std::remove_pointer_t<decltype(face)>;
-    X.vi = vi_d;
-    X.afm = S.d_afm;
-    X.mfa = S.d_mfa;
-    X.fxy = static_cast<F*>(S.d_face[0]);
-    X.fxz = static_cast<F*>(S.d_face[1]);
-    X.fyz = static_cast<F*>(S.d_face[2]);
-    X.nx = S.dims.ncell_x;
-    X.ny = S.dims.ncell_y;
-    X.nz = S.dims.ncell_z;
-    X.ne = S.dims.ne;
-    X.na = S.dims.na;
-    X.ngp = S.ngp;
-    P.tasks = S.d_tasks;
-    P.ntask = S.sched.ntask();
-    P.sy.sync = S.d_sync;
-    P.sy.timeout_ns = S.timeout_ns;
-  };
-  if (S.var.fn) {
-    Fp64Params P;
-    fill(P.pr, P, (double*)nullptr);
-    P.pr.vo = vo_d;
-    S.var.fn<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
+  if (S.var.fn && S.autotune && !S.tuned) {
+    // First sweep of an autotuning sweeper: the same sweep with each tile
+    // shape (each writes all of vo), timed on the stream; the faster shape
+    // is kept for every later sweep.
+    S.tuned = true;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    for (auto& e : ev)
+      if ((rc = cuda_check(cudaEventCreate(&e), "autotune event"))) return rc;
+    cudaEventRecord(ev[0], stream);
+    rc = launch_fp64(S, S.var, S.d_tasks, S.sched.ntask(), S.grid, vo_d, vi_d, stream);
+    if (!rc) rc = cuda_check(cudaEventRecord(ev[1], stream), "autotune event");
+    if (!rc) rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
+                             "status copy");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(stream), "autotune sweep");
+    if (!rc && S.h_status[SY_ERROR] == 0) {
+      rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync");
+      if (!rc) rc = launch_fp64(S, S.alt.var, S.alt.d_tasks, S.alt.sched.ntask(), S.alt.grid, vo_d, vi_d, stream);
+      if (!rc) rc = cuda_check(cudaEventRecord(ev[2], stream), "autotune event");
+      if (!rc) rc = cuda_check(cudaEventSynchronize(ev[2]), "autotune sweep");
+      if (!rc) {
+        cudaEventElapsedTime(&S.tune_ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&S.tune_ms[1], ev[1], ev[2]);
+        if (S.tune_ms[1] < S.tune_ms[0]) {
+          std::swap(S.var, S.alt.var);
+          std::swap(S.sched, S.alt.sched);
+          std::swap(S.gp_block, S.alt.gp_block);
+          std::swap(S.d_tasks, S.alt.d_tasks);
+          std::swap(S.grid, S.alt.grid);
+          std::swap(S.tune_ms[0], S.tune_ms[1]);
+        }
+      }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+  } else if (S.var.fn) {
+    if ((rc = launch_fp64(S, S.var, S.d_tasks, S.sched.ntask(), S.grid, vo_d, vi_d, stream))) return rc;
   } else {
-    MixParams P;
-    fill(P, P, (float*)nullptr);
-    P.part = S.d_part;
-    P.state = S.part_elems / NOCTANT;
-    if ((rc = encode_state_map(&P.tm_vi, vi_d, S.dims, &P.vbox_bytes))) return rc;
-    S.var.mix<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
-    if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
-    reduce_octant_partials<<<S.nsm * 8, 256, 0, stream>>>(vo_d, S.d_part, P.state);
+    if ((rc = launch_mixed(S, vo_d, vi_d, stream))) return rc;
   }
-  if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
                        "status copy")))
     return rc;
-  S.nlaunch = S.var.mix ? 2 : 1;
+  const int npass = (S.dims.na + pass_angles(S) - 1) / pass_angles(S);
+  S.nlaunch = (S.var.mix ? 2 : 1) * npass;
   return MSB_OK;
 }
 
@@ -395,11 +547,17 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   sweeper->precision = Arguments_consume_int_or_default(args, "--precision", 0);
   if (sweeper->precision < 0 || sweeper->precision > 2)
     return msb::set_error(MSB_ERR_ARG, "--precision must be 0 (FP64), 1 (mixed, FP16 halves) or 2 (mixed, BF16 halves)");
+  // tile shape of the FP64 sweep (cell columns per CTA): 0 = default, 42 = 4 x 2, 24 = 2 x 4
+  const int tile = Arguments_consume_int_or_default(args, "--tile", 0);
+  if (tile != 0 && tile != 42 && tile != 24) return msb::set_error(MSB_ERR_ARG, "--tile must be 0, 42 or 24");
+  // 1: the first sweep times both FP64 tile shapes and keeps the faster
+  const int autotune = Arguments_consume_int_or_default(args, "--autotune", 0);
+  if (autotune != 0 && autotune != 1) return msb::set_error(MSB_ERR_ARG, "--autotune must be 0 or 1");
   (void)env;
 
   std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
   if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
-  const int rc = msb::impl_create(*S, dims, sweeper->precision);
+  const int rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0);
   if (rc) return rc;
   sweeper->impl_ = S.release();
   return MSB_OK;
@@ -466,6 +624,16 @@ extern "C" int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int*
   if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
   if (ntask) *ntask = S->sched.ntask();
   if (nlaunch) *nlaunch = S->nlaunch;
+  return MSB_OK;
+}
+
+extern "C" int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_chosen, float* ms_other) {
+  const SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  if (tx) *tx = S->var.tx;
+  if (ty) *ty = S->var.ty;
+  if (ms_chosen) *ms_chosen = S->tuned ? S->tune_ms[0] : 0.f;
+  if (ms_other) *ms_other = S->tuned ? S->tune_ms[1] : 0.f;
   return MSB_OK;
 }
 

@@ -141,8 +141,13 @@ def test_unsupported_sizes_are_reported():
 @pytest.mark.parametrize("flags,d,code", [
     ("--precision 3", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),          # no such precision
     ("--precision -1", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),
-    ("--precision 1", (4, 4, 4, 2, 16, 64), msb.MSB_ERR_UNSUPPORTED),  # mixed kernels take na <= 32
+    ("--precision 1", (4, 4, 4, 2, 16, 129), msb.MSB_ERR_UNSUPPORTED),  # na <= 128 (four 32-angle passes)
     ("--precision 2", (4, 4, 4, 2, 12, 32), msb.MSB_ERR_UNSUPPORTED),  # NM 12
+    ("--tile 33", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),              # tile shapes: 0, 42, 24
+    ("--autotune 2", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),
+    ("--tile 24 --precision 1", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_UNSUPPORTED),  # mixed: one 4 x 4 tile
+    ("--tile 24", (4, 4, 4, 2, 16, 129), msb.MSB_ERR_UNSUPPORTED),     # na <= 128
+    ("--autotune 1 --precision 1", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_UNSUPPORTED),  # FP64 only
 ])
 def test_precision_flag_checks(flags, d, code):
     L = msb.lib()

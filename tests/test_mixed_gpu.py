@@ -10,6 +10,8 @@ than bit for bit:
   error of the split products dominates.  FP16 halves carry a 22-bit
   significand per operand, BF16 halves 16 bits:
   max |vo - vo_oracle| / max |vo_oracle| <= 1e-6 (FP16) and <= 2e-5 (BF16).
+* na > 32 is swept in 32-angle passes whose octant sums add up in vo
+  (angles are independent in the sweep); the same tolerances.
 * the built-in problem: its faces are large integers that cancel in the
   second transform, so the FP32 face recurrence limits the error to about
   1e-5 of max |vo| whatever the 16-bit format: max-rel <= 5e-5, and the
@@ -52,6 +54,9 @@ def rel_errors(vo, ref):
 
 BUILTIN = [
     (1, 1, 1, 1, 32, 16),
+    (3, 2, 3, 3, 33, 16),   # na > 32: one pass per 32 angles, the last one ragged
+    (4, 3, 2, 2, 128, 16),
+    (2, 3, 4, 3, 70, 4),
     (2, 1, 2, 3, 7, 16),
     (5, 4, 5, 3, 7, 4),
     (3, 4, 2, 5, 32, 16),
@@ -80,6 +85,9 @@ RANDOM = [
     (5, 5, 5, 4, 32, 4, 3),
     (6, 3, 5, 2, 24, 8, 4),
     (7, 6, 9, 6, 32, 16, 5),
+    (3, 4, 3, 3, 64, 16, 6),   # two 32-angle passes
+    (4, 3, 3, 2, 128, 16, 7),  # four passes (the dense geometry's na)
+    (3, 3, 4, 3, 45, 8, 8),    # a ragged last pass
 ]
 
 

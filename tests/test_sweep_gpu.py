@@ -41,8 +41,9 @@ BUILTIN = [
     (4, 3, 5, 20, 32, 16),
     (5, 5, 5, 30, 33, 16),   # the reference's default flags
     (7, 6, 5, 4, 64, 16),
-    (6, 5, 4, 3, 100, 8),
+    (6, 5, 4, 3, 100, 8),    # na > 64: passes of 64 angles, later passes add to vo
     (4, 4, 4, 2, 128, 16),
+    (3, 4, 5, 3, 65, 16),    # a one-angle second pass
     (16, 16, 16, 16, 32, 4),  # the CPU-runnable headline case
 ]
 
@@ -69,6 +70,33 @@ def test_builtin_flags_invariant(extra):
     assert np.array_equal(vo0, vo1)
 
 
+@pytest.mark.parametrize("nx,ny,nz,ne,na,nm,extra", [
+    (5, 4, 5, 3, 7, 16, "--tile 24"),
+    (7, 6, 5, 4, 64, 16, "--tile 24"),
+    (9, 7, 6, 5, 32, 4, "--tile 42"),
+    (9, 7, 6, 5, 32, 16, "--autotune 1"),
+    (6, 5, 4, 3, 40, 8, "--autotune 1 --tile 24"),
+    (5, 4, 3, 3, 128, 16, "--tile 24"),      # two 64-angle passes
+    (4, 5, 3, 2, 100, 4, "--autotune 1"),    # a 64-angle and a 36-angle pass
+])
+def test_tile_shapes_bitexact(nx, ny, nz, ne, na, nm, extra):
+    # the 2 x 4 tile (and the autotuned choice, whose first sweep runs both
+    # shapes) gives the same bits as the oracle, sweep after sweep
+    with msb.Problem(flags(nx, ny, nz, ne, na, extra), nm=nm) as pb:
+        vi = pb.init_state()
+        vo1 = pb.sweep_host(vi)
+        vo2 = pb.sweep_host(vi)
+        t = pb.tile()
+    a, m = oracle.am_matrices(nm, na)
+    ref = oracle.sweep(nx, ny, nz, ne, nm, na, a, m, vi)
+    assert np.array_equal(vo1, ref) and np.array_equal(vo2, ref)
+    assert (t["tx"], t["ty"]) in ((4, 2), (2, 4))
+    if "--autotune 1" in extra:
+        assert 0.0 < t["ms_chosen"] <= t["ms_other"]
+    elif "--tile 24" in extra:
+        assert (t["tx"], t["ty"]) == (2, 4)
+
+
 RANDOM = [
     (3, 2, 4, 3, 16, 16),
     (5, 4, 3, 4, 32, 16),
@@ -76,6 +104,7 @@ RANDOM = [
     (6, 3, 5, 2, 64, 8),
     (3, 5, 4, 3, 128, 16),
     (5, 5, 5, 4, 32, 4),
+    (4, 3, 4, 3, 97, 8),
 ]
 
 
