@@ -47,20 +47,26 @@ WORKLOAD = (f"minisweep KBA sweep, {NX}x{NY}x{NZ} cells, ne {NE}, na {NA}, NM {N
             f"nblock_z {NBLOCK_Z}, niterations {NITER}, built-in Quantities, FP64 plain")
 
 
-def updates_per_sweep(nx=NX, ny=NY, nz=NZ, ne=NE, na=NA) -> int:
+# Sizes default to the module's workload at call time (--case small changes it).
+def updates_per_sweep(nx=None, ny=None, nz=None, ne=None, na=None) -> int:
+    nx, ny, nz, ne, na = (NX if nx is None else nx, NY if ny is None else ny, NZ if nz is None else nz,
+                          NE if ne is None else ne, NA if na is None else na)
     return nx * ny * nz * ne * na * 8
 
 
-def flops_per_sweep(nx=NX, ny=NY, nz=NZ, ne=NE, na=NA, nm=NM) -> float:
+def flops_per_sweep(nx=None, ny=None, nz=None, ne=None, na=None, nm=None) -> float:
     # the reference's flop model (runner.c:162-166): two transforms + 12 per solve
+    nx, ny, nz, ne, na, nm = (NX if nx is None else nx, NY if ny is None else ny, NZ if nz is None else nz,
+                              NE if ne is None else ne, NA if na is None else na, NM if nm is None else nm)
     state = nx * ny * nz * ne * nm * NU
     return state * 8 * 2.0 * na * 2 + nx * ny * nz * ne * na * NU * 8 * 12.0
 
 
-def config_dict(ne=NE) -> dict:
-    return {"workload": WORKLOAD, "ncell": [NX, NY, NZ], "ne_per_gpu": ne, "na": NA, "nm": NM, "nu": NU,
-            "nblock_z": NBLOCK_Z, "niterations": NITER,
-            "l2": "state arrays of 8.6 GB each, far above the 126 MB L2: no flush needed between steps"}
+def config_dict(ne=None) -> dict:
+    gb = NX * NY * NZ * NE * NM * NU * 8 / 1e9
+    return {"workload": WORKLOAD, "ncell": [NX, NY, NZ], "ne_per_gpu": NE if ne is None else ne, "na": NA,
+            "nm": NM, "nu": NU, "nblock_z": NBLOCK_Z, "niterations": NITER,
+            "l2": f"state arrays of {gb:.2f} GB each, far above the 126 MB L2: no flush needed between steps"}
 
 
 # ------------------------------------------------------------------ helpers
@@ -107,11 +113,16 @@ class Clocks:
 
 
 def measured_peaks() -> dict:
+    """HBM copy bandwidth and BF16 GEMM peaks measured on this GPU pool
+    (MEASURED_PEAKS.json), else an earlier measurement of the same pool's
+    B200s (6.65 TB/s, 1.59 PFLOP/s), marked as the fallback."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return json.load(f)
+            d = json.load(f)
+        d["source"] = "measured (MEASURED_PEAKS.json)"
+        return d
     except (OSError, ValueError):
-        return {}
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback (earlier measurement on this pool)"}
 
 
 def profile_traffic(kernel: str = "sweep_fp64_kernel") -> float | None:
@@ -299,6 +310,7 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
                                   "the FP64 oracle on a 1e-7 perturbation)",
                     "error_random_seed1234": {"max_rel": r_max, "normsq_rel": r_nsq},
                     "roofline": {"bound": "hbm", "achieved": hbm, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                                 "peak_source": peaks.get("source"),
                                  "frac": hbm / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
                                  "traffic": profile_traffic("sweep_mixed_kernel"),
                                  "algorithmic": "16 x state bytes per sweep (vi read + vo write) / mean sweep "
@@ -579,7 +591,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                     "algorithmic": "reference flop model (runner.c:162-166) %.4g flop per sweep / mean sweep "
                                    "kernel time %.2f ms" % (flops_per_sweep(), ms_sweep),
                     "hbm_view": {"achieved_gbs": hbm_bytes / (ms_sweep * 1e-3) / 1e9,
-                                 "peak_gbs": peaks.get("hbm_gbs"),
+                                 "peak_gbs": peaks.get("hbm_gbs"), "peak_source": peaks.get("source"),
                                  "note": "algorithmic bytes 16 x state (vi read + vo write); the FP64 path is "
                                          "FP64-compute-bound, not HBM-bound"}}
         if rank == 0:
