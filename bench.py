@@ -19,8 +19,11 @@ with problems/s and the per-problem completion latency (p50 / p99).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank sweeps its own 64-group slice (energy groups are
-independent: no data exchange); the per-GPU work is fixed, so scaling is weak.
+Under torchrun rank r sweeps groups [64 r, 64 r + 64) of a 64 N-group problem
+(`--ie_base 64 r`: its own arrays, global group indices in the initial state
+and boundary fluxes); energy groups are independent, so the only exchange is
+the all-reduce of the two FP64 checksums (and the max of the timings).  The
+per-GPU work is fixed, so scaling is weak.
 The reference arm times the reference's own OpenMP CPU sweep (built from its
 sources into oracle/_ref) on the host cores, rank 0 only.
 """
@@ -41,6 +44,7 @@ if ROOT not in sys.path:
 
 NX = NY = NZ = 64
 NE, NA, NM, NU, NBLOCK_Z, NITER = 64, 32, 16, 4, 8, 10
+IE_BASE = 0  # under torchrun: global index of this rank's first energy group
 METRIC = "cell-angle-group updates/s, FP64 plain vs mixed-precision at stated error"
 UNIT = "updates/s"
 WORKLOAD = (f"minisweep KBA sweep, {NX}x{NY}x{NZ} cells, ne {NE}, na {NA}, NM {NM}, NU {NU}, "
@@ -244,12 +248,12 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
                 e.record(st)
                 evs.append(e)
 
-        pb.init_state_device(va.data_ptr())
+        pb.init_state_device(va.data_ptr(), IE_BASE)
         torch.cuda.synchronize()
         for _ in range(args.warmup):
             step()
         pb.sync()
-        pb.init_state_device(va.data_ptr())
+        pb.init_state_device(va.data_ptr(), IE_BASE)
         torch.cuda.synchronize()
         clocks = Clocks(torch.cuda.current_device())
         clocks.start()
@@ -269,7 +273,7 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
         value = updates_per_sweep() * NITER * args.steps * world / elapsed
         # ---- error on the built-in problem: FP64 leaves the state unchanged
         # (vo == vi exactly), so the reference result is the initial state
-        pb.init_state_device(va.data_ptr())
+        pb.init_state_device(va.data_ptr(), IE_BASE)
         pb.sweep_device(vb.data_ptr(), va.data_ptr())
         pb.sync()
         torch.cuda.synchronize()
@@ -335,7 +339,8 @@ def measure_dense(args, dev, world: int, local_rank: int) -> dict | None:
     from minisweep_b200.parallel import max_over_ranks
 
     nx, ny, nz, ne, na, nm, nbz = 32, 32, 96, 128, 128, 16, 12
-    fl = f"--ncell_x {nx} --ncell_y {ny} --ncell_z {nz} --ne {ne} --na {na} --nblock_z {nbz}"
+    ie_base = ne * int(os.environ.get("RANK", "0"))  # this rank's energy-group slice
+    fl = f"--ncell_x {nx} --ncell_y {ny} --ncell_z {nz} --ne {ne} --na {na} --nblock_z {nbz} --ie_base {ie_base}"
     upd = nx * ny * nz * ne * na * 8
     flops = flops_per_sweep(nx, ny, nz, ne, na, nm)
     out = {"workload": f"{nx}x{ny}x{nz} cells, ne {ne}, na {na}, NM {nm}, NU {NU}, nblock_z {nbz}, built-in "
@@ -349,7 +354,7 @@ def measure_dense(args, dev, world: int, local_rank: int) -> dict | None:
             if va is None:
                 va = torch.empty(pb.nstate, dtype=torch.float64, device=dev)
                 vb = torch.empty_like(va)
-            pb.init_state_device(va.data_ptr())
+            pb.init_state_device(va.data_ptr(), ie_base)
             torch.cuda.synchronize()
             st = torch.cuda.ExternalStream(pb.stream) if pb.stream else torch.cuda.current_stream()
             pb.sweep_device(vb.data_ptr(), va.data_ptr())
@@ -495,7 +500,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     import torch
 
     import minisweep_b200 as msb
-    from minisweep_b200.parallel import max_over_ranks
+    from minisweep_b200.parallel import max_over_ranks, sum_norms
 
     dist = None
     if world > 1:
@@ -511,15 +516,19 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
         if dist is not None:
             dist.barrier()
 
+    # rank r sweeps groups [64 r, 64 r + 64) of a 64 N-group problem: its own
+    # arrays, the global group index in the initial state and boundary fluxes
+    global IE_BASE
+    IE_BASE = NE * rank
     flags = (f"--ncell_x {NX} --ncell_y {NY} --ncell_z {NZ} --ne {NE} --na {NA} --nblock_z {NBLOCK_Z} "
-             f"--niterations {NITER}")
+             f"--niterations {NITER} --ie_base {IE_BASE}")
     # --autotune 1: the first (warm-up) sweep times both FP64 tile shapes and
     # keeps the faster for every later sweep
     pb = msb.Problem(flags + " --autotune 1", nm=NM)
     n = pb.nstate
     va = torch.empty(n, dtype=torch.float64, device=dev)
     vb = torch.empty(n, dtype=torch.float64, device=dev)
-    pb.init_state_device(va.data_ptr())
+    pb.init_state_device(va.data_ptr(), IE_BASE)
     stream = torch.cuda.ExternalStream(pb.stream)
     torch.cuda.synchronize()
     peak_dmma, peak_dfma = msb.fp64_peak(5)
@@ -561,12 +570,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     barrier()
 
     # correctness of the timed result (built-in Quantities: vo == vi exactly)
-    normsq, normsqdiff = pb.norms_device(va.data_ptr(), vb.data_ptr())
+    normsq, normsqdiff = sum_norms(*pb.norms_device(va.data_ptr(), vb.data_ptr()))
     mixed = measure_mixed(args, pb, flags, va, vb, stream, dev, world, ms_fp64=None)
     closed = None
     try:
         import oracle
-        closed = oracle.normsq_closed_form(NX, NY, NZ, NE, NM)
+        closed = oracle.normsq_closed_form(NX, NY, NZ, NE * world, NM)
     except Exception:  # the oracle is only the checker; the number stands without it
         pass
 
@@ -608,7 +617,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                     "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                     "data": "synthetic: the reference's built-in deterministic Quantities (index-derived state, "
                             "faces and transform matrices)",
-                    "config": dict(config_dict(), parallelism=f"{world} GPU(s) x 64-group slice, no exchange",
+                    "config": dict(config_dict(), parallelism=f"{world} GPU(s), each an energy-group slice of 64 "
+                                                              f"groups of a {NE * world}-group problem; checksums "
+                                                              "all-reduced (2 FP64 scalars), no other exchange",
                                    tile={"cells_per_cta": [tile["tx"], tile["ty"]],
                                          "autotune_first_sweep_ms": {"chosen": tile["ms_chosen"],
                                                                      "other": tile["ms_other"]}}),
@@ -619,7 +630,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                     "mixed_target": "mixed precision >= 2x the FP64 sweep at <= 1e-5 relative normsq error "
                                     "against it",
                     "check": {"normsq": normsq, "normsqdiff": normsqdiff, "normsq_closed_form": closed,
-                              "pass": normsqdiff == 0.0 and (closed is None or normsq == closed)},
+                              "pass": normsqdiff == 0.0 and (closed is None or (
+                                  normsq == closed if world == 1 else abs(normsq - closed) <= 1e-12 * closed)),
+                              "scope": f"all {NE * world} groups: per-rank checksums all-reduced (SUM)"},
                     "ms_per_sweep_kernel": ms_sweep,
                     "batched": batched,
                     "dense_case": dense}
@@ -633,7 +646,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
         return finish(None)
     host_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
     host_out = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    pb.init_state_device(va.data_ptr())
+    pb.init_state_device(va.data_ptr(), IE_BASE)
     torch.cuda.synchronize()
     host_in.copy_(va)
     del va, vb

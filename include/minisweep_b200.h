@@ -330,6 +330,11 @@ int msb_state_norms_device(const double* vi_d, const double* vo_d, size_t n,
                            double* normsq, double* normsqdiff, Env* env);
 /* Device-side built-in initial state (same values as initialize_state). */
 int msb_initialize_state_device(double* v_d, Dimensions dims, Env* env);
+/* The same for an energy-group slice: the array's group ie is global group
+ * ie_base + ie (no reference counterpart; the reference never splits the
+ * groups across processes, Quantities_init_state at quantities_testing.h:60-90
+ * is its per-element formula). */
+int msb_initialize_state_slice_device(double* v_d, Dimensions dims, int ie_base, Env* env);
 /* Kernel statistics of the last sweep: number of tasks, kernel launches. */
 int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int* nlaunch);
 /* Tile shape (cell columns per CTA) the sweeper uses and, with --autotune 1,

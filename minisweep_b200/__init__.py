@@ -121,6 +121,7 @@ def lib() -> ctypes.CDLL:
                                    P(ctypes.c_float)]
         L.msb_state_norms_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, P(D), P(D), P(Env)]
         L.msb_initialize_state_device.argtypes = [ctypes.c_void_p, Dimensions, P(Env)]
+        L.msb_initialize_state_slice_device.argtypes = [ctypes.c_void_p, Dimensions, ctypes.c_int, P(Env)]
         L.msb_schedule_tasks.argtypes = [ctypes.c_int] * 7 + [P(ctypes.c_int), ctypes.c_longlong]
         L.msb_schedule_tasks.restype = ctypes.c_longlong
         L.msb_batch_create.argtypes = [P(ctypes.c_void_p), P(ProblemDesc), ctypes.c_int, ctypes.c_int,
@@ -276,8 +277,11 @@ class Problem:
                                             ctypes.byref(s), ctypes.byref(d), ctypes.byref(self.env)))
         return s.value, d.value
 
-    def init_state_device(self, v_ptr: int) -> None:
-        _check(lib().msb_initialize_state_device(ctypes.c_void_p(v_ptr), self.dims, ctypes.byref(self.env)))
+    def init_state_device(self, v_ptr: int, ie_base: int = 0) -> None:
+        """Built-in initial state on the device; with ie_base, of the energy-group
+        slice whose group 0 is global group ie_base."""
+        _check(lib().msb_initialize_state_slice_device(ctypes.c_void_p(v_ptr), self.dims, ie_base,
+                                                       ctypes.byref(self.env)))
 
     @property
     def stream(self) -> int:

@@ -523,6 +523,7 @@ int upload_batch(BatchImpl& B) {
     q.ngp = P.ngp;
     q.ia_base = 0;
     q.vo_add = 0;
+    q.ie_base = 0;
   }
   if ((rc = upload(&B.d_tasks, B.rec, "batch tasks"))) return rc;
   if ((rc = upload(&B.d_task_prob, B.task_prob, "batch task problems"))) return rc;

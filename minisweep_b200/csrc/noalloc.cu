@@ -283,6 +283,7 @@ extern "C" int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double*
   P.pr.ngp = ngp;
   P.pr.ia_base = 0;
   P.pr.vo_add = 0;
+  P.pr.ie_base = 0;
   P.sy.sync = sync;
   P.sy.timeout_ns = 4000000000LL;
   const int v = nm == 16 ? 1 : 0;

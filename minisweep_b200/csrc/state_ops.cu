@@ -75,8 +75,9 @@ __global__ void norms_final_kernel(const double* __restrict__ part, int nblk, do
 }
 
 // Built-in initial state (quantities_testing.h:60-90), one thread per element
-// pair in the reference layout.
-__global__ void init_state_kernel(double* __restrict__ v, int nx, int ny, int nz, int ne, int nm) {
+// pair in the reference layout; group ie of the array is global group
+// ie_base + ie (an energy-group slice of a larger problem).
+__global__ void init_state_kernel(double* __restrict__ v, int nx, int ny, int nz, int ne, int nm, int ie_base) {
   const size_t n = (size_t)nx * ny * nz * ne * nm * NU;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     size_t k = i;
@@ -86,7 +87,7 @@ __global__ void init_state_kernel(double* __restrict__ v, int nx, int ny, int nz
     const int iy = (int)(k % ny); k /= ny;
     const int ie = (int)(k % ne); k /= ne;
     const int iz = (int)k;
-    v[i] = (double)(1 + im) * (double)d_scale_space(ix, iy, iz) * (double)d_scale_energy(ie) *
+    v[i] = (double)(1 + im) * (double)d_scale_space(ix, iy, iz) * (double)d_scale_energy(ie_base + ie) *
            (double)d_scale_unknown(iu);
   }
 }
@@ -113,11 +114,17 @@ extern "C" int msb_state_norms_device(const double* vi_d, const double* vo_d, si
   return MSB_OK;
 }
 
-extern "C" int msb_initialize_state_device(double* v_d, Dimensions dims, Env* env) {
+extern "C" int msb_initialize_state_slice_device(double* v_d, Dimensions dims, int ie_base, Env* env) {
   cudaStream_t st = env ? (cudaStream_t)env->stream_kernel_faces_ : nullptr;
   if (dims.nm <= 0) return msb::set_error(MSB_ERR_ARG, "invalid nm");
-  msb::init_state_kernel<<<148 * 8, 256, 0, st>>>(v_d, dims.ncell_x, dims.ncell_y, dims.ncell_z, dims.ne, dims.nm);
+  if (ie_base < 0) return msb::set_error(MSB_ERR_ARG, "ie_base must be >= 0");
+  msb::init_state_kernel<<<148 * 8, 256, 0, st>>>(v_d, dims.ncell_x, dims.ncell_y, dims.ncell_z, dims.ne, dims.nm,
+                                                 ie_base);
   return msb::cuda_check(cudaGetLastError(), "init state launch");
+}
+
+extern "C" int msb_initialize_state_device(double* v_d, Dimensions dims, Env* env) {
+  return msb_initialize_state_slice_device(v_d, dims, 0, env);
 }
 
 extern "C" long long msb_schedule_tasks(int nx, int ny, int nz, int ne, int tx, int ty, int gp_block, int* out,

@@ -59,6 +59,7 @@ struct Fp64Prob {
   double* fyz;
   int nx, ny, nz, ne, na, ngp;
   int ia_base;  // angle index of the first angle of afm / mfa (a multiple of 64: passes over na > 64)
+  int ie_base;  // global index of group 0 (energy-group slices of a larger problem)
   int vo_add;   // nonzero: every phase adds to vo (the passes after the first)
 };
 
@@ -527,7 +528,8 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
     const double so_r = 1.0 / so;  // rounded, as the reference's 1/(1+octant)
     // boundary flux = (1+ia) 2^(ia&7) s_space s_energy s_unknown (1+oct):
     // exact small integers, so the per-lane factor is formed once per task
-    const double face_k = gval ? (double)d_scale_energy(g_col) * (double)d_scale_unknown(q & 3) * so : 0.0;
+    const double face_k =
+        gval ? (double)d_scale_energy(Q.ie_base + g_col) * (double)d_scale_unknown(q & 3) * so : 0.0;
     const int sp_xy = ix + 3 * iy + 2;  // log2 s_space(x, y, z) = (sp_xy + 7 z) & 3
     // state offsets (doubles) of this column: + zstep per plane
     const size_t col = (size_t)NM_ * NU * (ix + (size_t)Q.nx * iy);

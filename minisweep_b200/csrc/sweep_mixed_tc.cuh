@@ -81,6 +81,7 @@ struct MixParams {
   long long ntask;
   int nx, ny, nz, ne, na, ngp;
   int ia_base;     // angle index of the first angle of afm / mfa (32-angle passes over a larger na)
+  int ie_base;     // global index of group 0 (energy-group slices of a larger problem)
   int vbox_bytes;  // bytes one TMA box delivers (both groups; one group when ne == 1)
   SyncArgs sy;
 };
@@ -668,7 +669,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const int kb1 = mat_scale[2 * mb], kb2 = mat_scale[2 * mb + 1];
       const float so = (float)(1 + oct);
       const float so_r = 1.0f / so;
-      const float face_k = rowv ? (float)d_scale_energy(g_col) * (float)d_scale_unknown(u) * so : 0.0f;
+      const float face_k =
+          rowv ? (float)d_scale_energy(P.ie_base + g_col) * (float)d_scale_unknown(u) * so : 0.0f;
       const int sp_xy = ix + 3 * iy + 2;
       const size_t ent_z = (size_t)(oct * P.ngp + gp) * P.nz;
       const size_t ent_y = (size_t)(oct * P.ngp + gp) * P.ny;

@@ -202,6 +202,7 @@ struct SweeperImpl {
   bool tuned = false;
   AltPlan alt;
   float tune_ms[2] = {0.f, 0.f};  // first sweep: the chosen shape, the other shape
+  int ie_base = 0;                // --ie_base: global index of this sweeper's group 0
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
@@ -342,6 +343,7 @@ static void fill_params(const SweeperImpl& S, X& x, PP& P, const double* vi_d, c
   x.na = S.dims.na;
   x.ngp = S.ngp;
   x.ia_base = 0;
+  x.ie_base = S.ie_base;
   P.tasks = d_tasks;
   P.ntask = ntask;
   P.sy.sync = S.d_sync;
@@ -553,10 +555,15 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // 1: the first sweep times both FP64 tile shapes and keeps the faster
   const int autotune = Arguments_consume_int_or_default(args, "--autotune", 0);
   if (autotune != 0 && autotune != 1) return msb::set_error(MSB_ERR_ARG, "--autotune must be 0 or 1");
+  // energy-group slice of a larger problem: group ie of the arrays is global
+  // group ie_base + ie (one process per GPU, each sweeping its own groups)
+  const int ie_base = Arguments_consume_int_or_default(args, "--ie_base", 0);
+  if (ie_base < 0) return msb::set_error(MSB_ERR_ARG, "--ie_base must be >= 0");
   (void)env;
 
   std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
   if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
+  S->ie_base = ie_base;
   const int rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0);
   if (rc) return rc;
   sweeper->impl_ = S.release();

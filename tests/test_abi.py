@@ -148,6 +148,7 @@ def test_unsupported_sizes_are_reported():
     ("--tile 24 --precision 1", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_UNSUPPORTED),  # mixed: one 4 x 4 tile
     ("--tile 24", (4, 4, 4, 2, 16, 129), msb.MSB_ERR_UNSUPPORTED),     # na <= 128
     ("--autotune 1 --precision 1", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_UNSUPPORTED),  # FP64 only
+    ("--ie_base -2", (4, 4, 4, 2, 16, 32), msb.MSB_ERR_ARG),           # first global group of a slice
 ])
 def test_precision_flag_checks(flags, d, code):
     L = msb.lib()

@@ -163,3 +163,40 @@ def test_timeout_reports_error_and_recovers():
         vo = pb.sweep_host(vi)
         assert np.array_equal(vo, vi)
         assert saw_timeout or True  # a schedule that never had to wait is also fine
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_energy_slices_match_full_problem(prec):
+    # The multi-GPU decomposition on one GPU: a 6-group problem swept whole
+    # and as two energy-group slices (groups 0-3 and 4-5, --ie_base 4), each
+    # slice with its own arrays and device-built initial state.  Groups are
+    # independent in the sweep, so each slice equals its groups of the whole
+    # sweep (FP64: bit for bit; mixed: the rows of a group pair do not mix,
+    # so the same bits too), and the slices' checksums add up to the whole's.
+    nx, ny, nz, ne, na, nm = 5, 4, 6, 6, 32, 16
+    dev = torch.device("cuda:0")
+
+    def sweep(ne_s, ie_base):
+        with msb.Problem(flags(nx, ny, nz, ne_s, na, f"--ie_base {ie_base} --precision {prec}"), nm=nm) as pb:
+            vi = torch.empty(pb.nstate, dtype=torch.float64, device=dev)
+            vo = torch.empty_like(vi)
+            pb.init_state_device(vi.data_ptr(), ie_base)
+            torch.cuda.synchronize()
+            pb.sweep_device(vo.data_ptr(), vi.data_ptr())
+            pb.sync()
+            s, d = pb.norms_device(vi.data_ptr(), vo.data_ptr())
+            return vi.cpu().numpy().reshape(nz, ne_s, -1), vo.cpu().numpy().reshape(nz, ne_s, -1), s, d
+
+    vi_f, vo_f, s_f, d_f = sweep(ne, 0)
+    parts = [sweep(4, 0), sweep(2, 4)]
+    vi_s = np.concatenate([p[0] for p in parts], axis=1)
+    vo_s = np.concatenate([p[1] for p in parts], axis=1)
+    assert np.array_equal(vi_s, vi_f)
+    assert np.array_equal(vo_s, vo_f)
+    # checksums: exact sums of integers for the FP64 sweep; the mixed result's
+    # partial sums come in another order
+    tol = 0.0 if prec == 0 else 1e-12
+    assert abs(sum(p[2] for p in parts) - s_f) <= tol * s_f
+    assert abs(sum(p[3] for p in parts) - d_f) <= tol * max(d_f, 1.0)
+    if prec == 0:
+        assert d_f == 0.0 and s_f == oracle.normsq_closed_form(nx, ny, nz, ne, nm)
