@@ -466,6 +466,31 @@ def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict |
             seq_ms += e0.elapsed_time(e1)
             if i < 8:  # the batched result equals the problem's own Sweeper bit for bit
                 exact = exact and bool(torch.equal(ref, vos[i]))
+    # mixed precision on the same problems: one mixed Sweeper per problem, one
+    # after another (the persistent batched kernel sweeps in FP64 only); the
+    # FP64 sweep of the built-in problem returns its input, so the error of
+    # each mixed result is measured against vi
+    mix_ms, mix_done, mix_rel, mix_nsq = [], [], 0.0, 0.0
+    for i, q in enumerate(probs):
+        fl = f"--ncell_x {q['ncell_x']} --ncell_y {q['ncell_y']} --ncell_z {q['ncell_z']} --ne {q['ne']} --na {q['na']}"
+        with msb.Problem(fl + " --precision 1", nm=q["nm"]) as pb1:
+            out = torch.empty_like(vis[i])
+            st1 = torch.cuda.ExternalStream(pb1.stream) if pb1.stream else torch.cuda.current_stream()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st1)
+            pb1.sweep_device(out.data_ptr(), vis[i].data_ptr())
+            e1.record(st1)
+            pb1.sync()
+            mix_ms.append(e0.elapsed_time(e1))
+            mix_done.append(sum(mix_ms))
+            ref = vis[i]
+            mix_rel = max(mix_rel, (torch.max(torch.abs(out - ref)) / torch.max(torch.abs(ref))).item())
+            nr = torch.sum(ref * ref)
+            mix_nsq = max(mix_nsq, abs((torch.sum(out * out) - nr) / nr).item())
+            del out
+    mix_total = max_over_ranks(sum(mix_ms) / 1e3) * 1e3
     batch_ms = max_over_ranks(min(ms) / 1e3) * 1e3
     seq_ms = max_over_ranks(seq_ms / 1e3) * 1e3
     upd = sum(q["ncell_x"] * q["ncell_y"] * q["ncell_z"] * q["ne"] * q["na"] * 8 for q in W)
@@ -485,6 +510,16 @@ def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict |
             "unbatched_ms": seq_ms,
             "speedup_vs_unbatched": seq_ms / batch_ms,
             "exact_vs_sweeper": exact,
+            "mixed_sequential": {
+                "precision": 1, "format": "FP16 hi+lo halves", "value": len(W) / (mix_total / 1e3),
+                "unit": "problems/s", "ms_total": mix_total,
+                "latency_ms": {"p50": float(np.percentile(mix_done, 50)), "p99": float(np.percentile(mix_done, 99)),
+                               "definition": "completion time of each problem counted from the start of the "
+                                             "sequence (rank 0's share)"},
+                "error_vs_fp64_max_over_problems": {"max_rel": mix_rel, "normsq_rel": mix_nsq},
+                "launches_per_problem": "2 per 32-angle pass (sweep kernel + partial sum)",
+                "note": "one mixed-precision Sweeper per problem, swept one after another: the persistent "
+                        "batched kernel sweeps in FP64 only"},
             "problems_per_rank": len(probs), "ntask": info["ntask"],
             "classes": [{"nm": c["nm"], "angle_chunks": c["nch"], "tile": list(c["tile"]), "ntask": c["ntask"]}
                         for c in info["classes"]],
