@@ -197,7 +197,7 @@ struct MixCfg {
   static constexpr int NW = 8;              // compute warps: tile row x angle half
   static constexpr int NT = (NW + 3) * 32;  // + loader, publisher, MMA issuer
   static constexpr int KP = 16;             // moments, padded to one MMA K-step
-  static constexpr int NA = 32;             // angles per MMA (na <= 32)
+  static constexpr int NA = 32;             // angles per MMA: one pass (larger na: one pass per 32)
   static constexpr int EB = 1024;           // bytes per face entry: 8 rows x 32 floats
   // vi / previous-vo blocks: 128 rows of NM doubles; one cell (2 groups x 4
   // unknowns = 8 rows) is one TMA box, swizzled: the 16-byte chunk j of row r
