@@ -146,7 +146,8 @@ int plan_problem(ProbPlan& P, int nsm) {
   const msb_problem& d = P.d;
   P.nch = (d.na + 31) / 32;
   P.ngp = (d.ne + 1) / 2;
-  const int gpb = pick_gp_block(d.ncell_x, d.ncell_y, P.ngp, P.tx, P.ty, 2 * nsm);
+  // the same task window as a single problem's schedule (4 x SMs)
+  const int gpb = pick_gp_block(d.ncell_x, d.ncell_y, P.ngp, P.tx, P.ty, 4 * nsm);
   int rc = build_schedule(d.ncell_x, d.ncell_y, d.ncell_z, P.ngp, P.tx, P.ty, gpb, P.sched);
   if (rc) return rc;
   const size_t per = (size_t)NOCTANT * P.ngp * (size_t)P.nch * 256 * sizeof(double);
