@@ -145,27 +145,30 @@ def reference_binary() -> str | None:
 
 
 def cpu_sample(ne_sample: int | None = None):
-    """One bounded run of the reference OpenMP sweep on the host cores.
-    Returns (updates/s, seconds, threads, description) or None."""
+    """One run of the reference OpenMP sweep on the host cores: one sweep of
+    the benchmark problem (all NE groups, --nthread_e = the host cores), or of
+    its first ne_sample groups.  Returns (updates/s, seconds, threads,
+    description) or None."""
     binp = reference_binary()
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    nthr = max(1, min(NE, cores or 1))
-    ne = ne_sample or nthr
+    ne = ne_sample or NE
+    nthr = max(1, min(ne, cores or 1))
     if binp is None:
         return None
     env = dict(os.environ, OMP_NUM_THREADS=str(nthr), OMP_PROC_BIND="true")
     args = [binp, "--ncell_x", str(NX), "--ncell_y", str(NY), "--ncell_z", str(NZ), "--ne", str(ne),
             "--na", str(NA), "--nblock_z", str(NBLOCK_Z), "--nthread_e", str(nthr), "--nthread_octant", "1",
             "--niterations", "1"]
-    out = subprocess.run(args, env=env, capture_output=True, text=True, timeout=900).stdout
+    out = subprocess.run(args, env=env, capture_output=True, text=True, timeout=1500).stdout
     m = re.search(r"time:\s*([0-9.]+)", out)
     ok = "PASS" in out
     if not m or not ok:
         return None
     sec = float(m.group(1))
     u = updates_per_sweep(ne=ne)
-    desc = (f"reference OpenMP sweep (oracle/_ref/sweep_omp_nm{NM}, --nthread_e {nthr}), "
-            f"{NX}^3 cells x ne {ne} x na {NA}, 1 sweep ({u:.3g} updates, {sec:.2f} s)")
+    desc = (f"reference OpenMP sweep (oracle/_ref/sweep_omp_nm{NM}, --nthread_e {nthr} --nthread_octant 1, "
+            f"OMP_PROC_BIND=true), {NX}^3 cells x ne {ne} x na {NA} x NM {NM}, nblock_z {NBLOCK_Z}, "
+            f"one sweep ({u:.3g} updates, {sec:.2f} s)")
     return u / sec, sec, nthr, desc
 
 
@@ -188,25 +191,36 @@ def cpu_sample_port():
 
 # ------------------------------------------------------------------ arms
 def run_reference(args, rank: int) -> int:
+    """The reference arm: the reference's own OpenMP sweep on the host cores,
+    on the GPU arm's problem (same config).  A timed step is one sweep of the
+    whole 64^3 x ne 64 problem (about 20 s on 16 cores; the metric is a rate
+    per sweep, the GPU arm's step runs the problem's 10 sweeps).  A CPU binary
+    has nothing to warm up beyond what every fresh process pays, so the warm-up
+    steps sweep a quarter of the groups."""
     if rank != 0:
         return 0
     vals, secs = [], []
     kind = "reference"
+    desc, nthr = "", 1
     for i in range(args.warmup + args.steps):
-        r = cpu_sample()
+        timed = i >= args.warmup
+        r = cpu_sample(None if timed else max(1, NE // 4))
         if r is None:
             kind = "port"
             r = cpu_sample_port()
-        if i >= args.warmup:
+        if timed:
             vals.append(r[0])
             secs.append(r[1])
-        nthr, desc = r[2], r[3]
+            nthr, desc = r[2], r[3]
     v = sorted(vals)[len(vals) // 2]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic: the reference's built-in deterministic Quantities", "config": config_dict(),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthr, "kind": kind, "sample": desc},
+            "step": "one sweep of the configured problem (its niterations are repeats of that sweep; "
+                    "value is the median per-step rate)",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthr, "kind": kind,
+                             "sample": desc + "; warm-up steps: ne %d" % max(1, NE // 4)},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -317,6 +331,9 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
                                  "peak_source": peaks.get("source"),
                                  "frac": hbm / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
                                  "traffic": profile_traffic("sweep_mixed_kernel"),
+                                 "traffic_source": "constant read from profiles/sweep_mixed_kernel.md: ncu DRAM "
+                                                   "bytes of one 32^3 x ne 32 sweep scaled x16; not measured in "
+                                                   "this run",
                                  "algorithmic": "16 x state bytes per sweep (vi read + vo write) / mean sweep "
                                                 "kernel time"}})
         pb.close()
@@ -630,6 +647,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
         roofline = {"bound": "tensor", "achieved": tf, "peak": peak_dmma, "unit": "TFLOP/s",
                     "frac": tf / peak_dmma if peak_dmma else None,
                     "traffic": traffic,
+                    "traffic_source": "constant read from profiles/sweep_fp64_kernel.md: ncu DRAM bytes of one "
+                                      "32^3 x ne 32 sweep scaled x16 to this workload; not measured in this run",
                     "peak_source": "FP64 mma.sync peak measured live by msb_measure_fp64_peak (MEASURED_PEAKS.json "
                                    "has no FP64 figure); FMA-pipe FP64 peak %.2f TF/s" % peak_dfma,
                     "algorithmic": "reference flop model (runner.c:162-166) %.4g flop per sweep / mean sweep "
@@ -641,7 +660,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
         if rank == 0:
             cpu = None
             if world == 1 and not args.no_cpu:
-                r = cpu_sample(ne_sample=None)
+                # a bounded sample for the GPU arm's own line: a quarter of the
+                # groups (the full problem is the reference arm's step)
+                r = cpu_sample(ne_sample=max(1, NE // 4))
                 kind = "reference"
                 if r is None:
                     r = cpu_sample_port()
@@ -652,12 +673,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                     "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                     "data": "synthetic: the reference's built-in deterministic Quantities (index-derived state, "
                             "faces and transform matrices)",
-                    "config": dict(config_dict(), parallelism=f"{world} GPU(s), each an energy-group slice of 64 "
-                                                              f"groups of a {NE * world}-group problem; checksums "
-                                                              "all-reduced (2 FP64 scalars), no other exchange",
-                                   tile={"cells_per_cta": [tile["tx"], tile["ty"]],
-                                         "autotune_first_sweep_ms": {"chosen": tile["ms_chosen"],
-                                                                     "other": tile["ms_other"]}}),
+                    "config": config_dict(),
+                    "step": f"one run of the configured problem: its {NITER} sweeps with the vi/vo swap",
+                    "parallelism": f"{world} GPU(s), each an energy-group slice of {NE} groups of a "
+                                   f"{NE * world}-group problem; checksums all-reduced (2 FP64 scalars), no other "
+                                   "exchange",
+                    "tile": {"cells_per_cta": [tile["tx"], tile["ty"]],
+                             "autotune_first_sweep_ms": {"chosen": tile["ms_chosen"], "other": tile["ms_other"]}},
                     "roofline": roofline, "cpu_baseline": cpu,
                     "e2e": e2e,
                     "clocks": clk, "gpu_launches": args.steps * NITER,

@@ -370,9 +370,14 @@ int msb_measure_fp64_peak(double* tflops_dmma, double* tflops_dfma, int reps);
  * Limits: NM 4 or 16, na <= 32, and the problem's scratch must fit the array
  * (about 10^3 cells x 8 groups); larger problems return MSB_ERR_ARG with the
  * bytes needed.  The first call on each device sets up (takes the array's
- * device address with that device current): make it before any stream
- * capture.  All calls share the array, which keeps the last call's contents;
- * calls that overlap, on the GPU or on the host, race. */
+ * device address with that device current).  Under CUDA's default lazy module
+ * loading the array's 32 MiB are committed on a device by that first call
+ * (at load time with CUDA_MODULE_LOADING=EAGER): a caller whose pool takes
+ * every free byte makes one call before creating the pool.  Every call reads
+ * the kernel's status back and synchronises `stream`, so no call may be made
+ * while `stream` is capturing a graph (refused with MSB_ERR_UNSUPPORTED).
+ * All calls share the array, which keeps the last call's contents; calls that
+ * overlap, on the GPU or on the host, race. */
 #define MSB_NOALLOC_SCRATCH_BYTES (32u << 20)
 int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double* a_from_m_d, const double* m_from_a_d,
                       int ncell_x, int ncell_y, int ncell_z, int ne, int nm, int na, void* stream);

@@ -271,6 +271,15 @@ class Problem:
     def sync(self) -> None:
         _check(lib().Sweeper_sync_status(ctypes.byref(self.sweeper), ctypes.byref(self.env)))
 
+    def state_norms(self, vi: np.ndarray, vo: np.ndarray):
+        """(normsq, normsqdiff) of host arrays by the library's get_state_norms
+        (the reference's loop order, array_operations.c:69-110)."""
+        s, d = ctypes.c_double(), ctypes.c_double()
+        DP = ctypes.POINTER(ctypes.c_double)
+        lib().get_state_norms(vi.ctypes.data_as(DP), vo.ctypes.data_as(DP), self.dims, NU, ctypes.byref(s),
+                              ctypes.byref(d), ctypes.byref(self.env))
+        return s.value, d.value
+
     def norms_device(self, vi_ptr: int, vo_ptr: int):
         s, d = ctypes.c_double(), ctypes.c_double()
         _check(lib().msb_state_norms_device(ctypes.c_void_p(vi_ptr), ctypes.c_void_p(vo_ptr), self.nstate,
@@ -321,6 +330,30 @@ class Problem:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def run_case(argstring: str, nm: int = 16):
+    """One run of the reference driver's Runner_run_case (runner.c:51-183) on
+    this library: the built-in initial state, --niterations sweeps through
+    Sweeper_sweep's host-in / host-out semantics with the vi/vo swap, then the
+    norms of the two host arrays.  Returns (normsq, normsqdiff)."""
+    with Problem(argstring, nm=nm) as pb:
+        vi = pb.init_state()
+        vo = np.zeros_like(vi)
+        for it in range(pb.niterations):
+            if it % 2 == 0:
+                vo = pb.sweep_host(vi)
+            else:
+                vi = pb.sweep_host(vo)
+        return pb.state_norms(vi, vo)
+
+
+def compare_runs(argstring1: str, argstring2: str, nm: int = 16) -> bool:
+    """The reference's compare_runs (runner.c:187-241): both runs must have
+    normsqdiff == 0 and the same normsq."""
+    n1, d1 = run_case(argstring1, nm)
+    n2, d2 = run_case(argstring2, nm)
+    return d1 == 0.0 and d2 == 0.0 and n1 == n2
 
 
 # ------------------------------------------------------------------ batches
@@ -435,15 +468,6 @@ class Batch:
         pred = np.zeros(max(npred, 1), dtype=np.int32)
         _check(min(0, L.msb_batch_scratch(self._h, None, None, None, pred.ctypes.data_as(IP), len(pred))))
         return off, nb, po, pred[:npred]
-
-    def tile(self) -> dict:
-        """Tile shape in use and, with --autotune 1, the first sweep's times of
-        the chosen and the other shape (ms)."""
-        tx, ty = ctypes.c_int(), ctypes.c_int()
-        a, b = ctypes.c_float(), ctypes.c_float()
-        _check(lib().Sweeper_tile(ctypes.byref(self.sweeper), ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(a),
-                                  ctypes.byref(b)))
-        return {"tx": tx.value, "ty": ty.value, "ms_chosen": a.value, "ms_other": b.value}
 
     def set_timeout_ns(self, ns: int) -> None:
         _check(lib().msb_batch_set_spin_limit(self._h, ns))

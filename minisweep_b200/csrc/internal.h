@@ -12,6 +12,10 @@
 
 namespace msb {
 
+// Time budget of one device-side wait (a dependency, a barrier phase) before
+// the sweep gives up with MSB_ERR_TIMEOUT.
+constexpr long long kDefaultTimeoutNs = 4000000000LL;  // 4 s
+
 int set_error(int code, const char* fmt, ...);
 #ifdef __CUDACC__
 int cuda_check(cudaError_t e, const char* what);

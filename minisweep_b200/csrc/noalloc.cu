@@ -12,19 +12,25 @@
 // Properties a caller must know:
 //   * The scratch array (MSB_NOALLOC_SCRATCH_BYTES, 32 MiB) is part of the
 //     library image: every GPU that loads the library holds it until exit.
+//     Under CUDA's default lazy module loading the array is committed on a
+//     device when this file's module is first used there, i.e. by the first
+//     call on that device (at load time with CUDA_MODULE_LOADING=EAGER), so a
+//     caller whose pool takes every free byte makes one call first.
 //   * Problems whose scratch does not fit are rejected with MSB_ERR_ARG and a
 //     message giving the bytes needed.  Supported: NM 4 or 16, na <= 32.
 //   * The first call on each device does the set-up: it takes the device
 //     address of the scratch array (cudaGetSymbolAddress, with that device
 //     current), sets the kernel's shared-memory limit and reads the SM count.
-//     Make that first call before any stream capture.
 //   * Every call shares the scratch array and the host-side schedule buffers,
 //     and the array keeps the last call's contents.  The progress counters are
 //     cleared at every call; the face planes need no clearing (every entry is
 //     written before it is read).  Calls that overlap -- on the GPU (different
 //     streams) or on the host (different threads) -- race: serialise them.
 //   * The call returns after the sweep has finished (it reads the kernel's
-//     status word), so its result is ready in vo_d.
+//     status word back and synchronises the stream), so its result is ready
+//     in vo_d.  That read-back cannot be captured in a CUDA graph: a call on
+//     a stream that is capturing is refused with MSB_ERR_UNSUPPORTED before
+//     anything is enqueued.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -220,6 +226,12 @@ extern "C" int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double*
     return set_error(MSB_ERR_UNSUPPORTED, "noalloc sweep: supports NM 4 or 16 and na <= 32 (got NM %d, na %d)",
                      nm, na);
   int dev = 0, rc;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if ((rc = cuda_check(cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap), "cudaStreamIsCapturing")))
+    return rc;
+  if (cap != cudaStreamCaptureStatusNone)
+    return set_error(MSB_ERR_UNSUPPORTED, "noalloc sweep: the stream is capturing; this call synchronises and "
+                                          "cannot be captured");
   if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
   if (dev < 0 || dev >= kMaxDevices) return set_error(MSB_ERR_UNSUPPORTED, "noalloc sweep: device index %d", dev);
   DeviceState& D = g_dev[dev];
@@ -285,7 +297,7 @@ extern "C" int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double*
   P.pr.vo_add = 0;
   P.pr.ie_base = 0;
   P.sy.sync = sync;
-  P.sy.timeout_ns = 4000000000LL;
+  P.sy.timeout_ns = kDefaultTimeoutNs;
   const int v = nm == 16 ? 1 : 0;
   const int grid = (int)std::min<long long>(ntask, (long long)D.nsm * D.occ[v]);
   const Kernel k = v ? kernel_for<16>() : kernel_for<4>();

@@ -116,8 +116,6 @@ Variant pick_variant(int nm, int na, int precision, int tile = 0) {
   }
 }
 
-constexpr long long kDefaultTimeoutNs = 4000000000LL;  // 4 s per wait
-
 // cuTensorMapEncodeTiled from the driver, through the runtime (no -lcuda).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;

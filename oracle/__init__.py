@@ -21,11 +21,17 @@ NOCTANT = 8
 _dp = ctypes.POINTER(ctypes.c_double)
 
 
+def reference_tree() -> str:
+    """The reference's source tree: $MINISWEEP_REF when set, else a checkout
+    named ``reference`` beside this repository (the Makefile's default too)."""
+    return os.environ.get("MINISWEEP_REF") or os.path.abspath(os.path.join(HERE, "..", "..", "reference"))
+
+
 def build(with_reference: bool | None = None) -> None:
     """Compile the C restatement (and the reference build when its tree exists)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
     if with_reference is None:
-        with_reference = os.path.isdir("/root/reference/src")
+        with_reference = os.path.isdir(os.path.join(reference_tree(), "src"))
     if with_reference:
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
         # the reference's driver programs linked with the product library

@@ -4,9 +4,11 @@ oracle/Makefile's `dropin` target compiles the reference's src/4_driver/
 runner.c + sweep.c and runner.c + tester.c against include/ and links them
 with libminisweep_b200.so in place of the reference's libsweeper.  Here they
 run on the GPU: `sweep` must print the reference's result line with PASS and
-the reference's normsq, and `tester` must pass its whole battery (the
-compare_runs pairs of tester.c, each requiring normsqdiff == 0 and equal
-normsq across two flag sets).
+the reference's normsq, and each `tester` build must pass its whole battery
+(the compare_runs pairs of tester.c, each requiring normsqdiff == 0 and equal
+normsq across two flag sets) with exactly the pair count the reference's own
+build of that configuration runs (measured on the reference's CPU builds:
+serial 54, OpenMP threads 981, OpenMP tasks 64, variants 2).
 """
 import os
 import re
@@ -54,9 +56,23 @@ def test_reference_sweep_driver_rejects_bad_flags():
     assert "Insist" in out.stderr
 
 
-def test_reference_tester_battery():
-    out = subprocess.run([binary("tester_b200_nm16")], capture_output=True, text=True, timeout=1200)
+# (binary, pairs): tester.c's batteries are chosen by the build macros of
+# the reference's configurations (tester.c:46-99 test_serial, :104-212
+# test_openmp, :217-285 test_openmp_tasks, :511-546 test_variants).
+BATTERIES = [
+    ("tester_b200_nm16", 2),
+    ("tester_b200_serial_nm16", 54),
+    ("tester_b200_serial_nm4", 54),
+    ("tester_b200_omp_nm4", 981),
+    ("tester_b200_omp_nm16", 981),
+    ("tester_b200_tasks_nm16", 64),
+]
+
+
+@pytest.mark.parametrize("name,pairs", BATTERIES)
+def test_reference_tester_battery(name, pairs):
+    out = subprocess.run([binary(name)], capture_output=True, text=True, timeout=1200)
     assert out.returncode == 0, out.stderr[-2000:]
     m = re.search(r"TESTS\s+(\d+)\s+PASSED\s+(\d+)\s+FAILED\s+(\d+)", out.stdout)
     assert m, out.stdout[-2000:]
-    assert int(m.group(1)) > 0 and m.group(1) == m.group(2) and int(m.group(3)) == 0
+    assert (int(m.group(1)), int(m.group(2)), int(m.group(3))) == (pairs, pairs, 0), out.stdout[-2000:]

@@ -86,9 +86,62 @@ def test_noalloc_refuses_sizes_beyond_the_array():
     f = noalloc()
     one = torch.zeros(8, dtype=torch.float64, device="cuda:0")
     p = one.data_ptr()
-    # 64^3 cells x 64 groups needs gigabytes of face planes
+    # 64^3 cells x 64 groups: more tasks than the static schedule holds
     rc = f(p, p, p, p, 64, 64, 64, 64, 16, 32, None)
     assert rc == msb.MSB_ERR_ARG
-    assert "scratch" in msb.last_error() or "schedule" in msb.last_error()
+    assert "schedule" in msb.last_error()
+    # 16^3 cells x 8 groups: 2048 tasks fit the schedule, but the face planes
+    # (3 x 16 MiB) do not fit the 32 MiB array
+    rc = f(p, p, p, p, 16, 16, 16, 8, 16, 32, None)
+    assert rc == msb.MSB_ERR_ARG
+    assert "bytes of scratch" in msb.last_error()
     rc = f(p, p, p, p, 4, 4, 4, 2, 8, 32, None)  # NM 8: not in this entry point
     assert rc == msb.MSB_ERR_UNSUPPORTED
+
+
+def test_noalloc_call_allocates_no_device_memory():
+    # After one call on the device (which commits the array), further calls
+    # -- here with another problem shape, so the schedule is rebuilt -- leave
+    # the device's free memory unchanged.
+    dev = torch.device("cuda:0")
+    shapes = [(6, 5, 7, 3), (8, 8, 8, 8)]
+    bufs = []
+    for nx, ny, nz, ne in shapes:
+        with msb.Problem(f"--ncell_x {nx} --ncell_y {ny} --ncell_z {nz} --ne {ne} --na 32", nm=16) as pb:
+            vi = pb.init_state()
+            a_h, m_h = pb.matrices()
+            bufs.append((torch.from_numpy(vi).to(dev), torch.empty(vi.size, dtype=torch.float64, device=dev),
+                         torch.from_numpy(a_h.copy()).to(dev), torch.from_numpy(m_h.copy()).to(dev)))
+    torch.cuda.synchronize()
+    f = noalloc()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def call(i):
+        nx, ny, nz, ne = shapes[i]
+        d_vi, d_vo, d_a, d_m = bufs[i]
+        assert f(d_vo.data_ptr(), d_vi.data_ptr(), d_a.data_ptr(), d_m.data_ptr(), nx, ny, nz, ne, 16, 32,
+                 stream) == msb.MSB_OK, msb.last_error()
+
+    call(0)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    call(1)
+    call(0)
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    assert torch.equal(bufs[0][1], bufs[0][0])  # the built-in problem is a fixed point of the sweep
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    dev = torch.device("cuda:0")
+    one = torch.zeros(8, dtype=torch.float64, device=dev)
+    p = one.data_ptr()
+    f = noalloc()
+    s = torch.cuda.Stream(dev)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        try:
+            rc = f(p, p, p, p, 4, 4, 4, 2, 16, 32, s.cuda_stream)
+        finally:
+            g.capture_end()
+    assert rc == msb.MSB_ERR_UNSUPPORTED
+    assert "capturing" in msb.last_error()
