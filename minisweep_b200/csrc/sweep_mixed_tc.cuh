@@ -18,8 +18,9 @@
 //   FP16 halves that is a 22-bit significand per operand (errors near FP32
 //   rounding); with BF16 halves 16 bits.  Quantities_solve
 //   (quantities_testing_kernels.h:337-447) runs in FP32 with fused
-//   multiply-adds; faces are stored in FP32.  vo is read, summed and written
-//   in FP64.
+//   multiply-adds except its last step, psi = sm * cc + vs, which is formed
+//   in FP64 (with the FP64 reciprocal 1 / (1 + octant)) and rounded once to
+//   FP32; faces are stored in FP32.  vo is read, summed and written in FP64.
 //
 // Tile and roles (one CTA, 10 warps)
 //   A task is a 4 x 4 tile of cell columns x one group pair.  MMA row
@@ -668,7 +669,9 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const int cbeg = a + b;
       const int kb1 = mat_scale[2 * mb], kb2 = mat_scale[2 * mb + 1];
       const float so = (float)(1 + oct);
-      const float so_r = 1.0f / so;
+      // 1 / (1 + octant) rounded in FP64, as the reference rounds it: the
+      // product with it is formed in FP64 (see the solve below)
+      const double so_rd = 1.0 / (double)(1 + oct);
       const float face_k =
           rowv ? (float)d_scale_energy(P.ie_base + g_col) * (float)d_scale_unknown(u) * so : 0.0f;
       const int sp_xy = ix + 3 * iy + 2;
@@ -802,7 +805,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         const float cxy = f_pow2(-1 - ((sp_xy + 7 * (iz - dz)) & 3));
         const float cxz = f_pow2(-2 - ((sp_xy - 3 * dy + 7 * iz) & 3));
         const float sx_r = f_pow2(-((sp_xy - dx + 7 * iz) & 3));
-        const float cc = so_r * f_pow2((sp_xy + 7 * iz) & 3);
+        const double ccd = so_rd * d_pow2((sp_xy + 7 * iz) & 3);
         // vs = D1a * 2^-(k1 + kb1) [+ D1b * 2^-(k1b + kb1)], each term in two
         // exact steps, the smaller factor first, so no intermediate leaves the
         // FP32 range unless the term itself does
@@ -875,7 +878,12 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             const float sm = __fmaf_rn(fyz[i], __fmul_rn(wz, sx_r), sab);
             float vs = __fmul_rn(__fmul_rn(v[i], vsc1), vsc2);
             if constexpr (C::SPLIT_K) vs = __fmaf_rn(__fmul_rn(vb[i], vbs1), vbs2, vs);
-            const float psi = __fmaf_rn(sm, cc, vs);
+            // psi = sm * cc + vs with one rounding from FP64: the FP64
+            // reciprocal of (1 + octant) and no FP32 rounding of the product
+            // (formed in FP32 -- with the FP32 reciprocal and product -- the
+            // cancellation of the large boundary fluxes in T2 amplifies that
+            // rounding up to 1e-4 relative in vo at na 64-128)
+            const float psi = __double2float_rn(__fma_rn((double)sm, ccd, (double)vs));
             v[i] = psi;
             pmax = fmaxf(pmax, fabsf(psi));
             carry[i] = __fmul_rn(psi, so);

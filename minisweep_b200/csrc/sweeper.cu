@@ -15,6 +15,7 @@
 #include <type_traits>
 
 #include "internal.h"
+#include "sweep_fp64_chain.cuh"
 #include "sweep_fp64_ws.cuh"
 #include "sweep_mixed_tc.cuh"
 
@@ -32,6 +33,7 @@ struct Variant {
   size_t smem = 0;
   size_t entry_bytes = 0;  // one face entry (octant, group pair, position)
   int tx = 0, ty = 0, nch = 0, threads = 0;
+  int pass = 64;  // angles swept per launch (na above it is swept in passes)
   bool valid() const { return fn || mix; }
   const void* func() const { return fn ? (const void*)fn : (const void*)mix; }
 };
@@ -54,6 +56,24 @@ Variant make_variant() {
   v.ty = TY;
   v.nch = NCH;
   v.threads = C::NT;
+  v.pass = 32 * NCH;
+  return v;
+}
+
+// The chained-wavefront FP64 kernel (sweep_fp64_chain.cuh): one 32-angle
+// chunk per pass.
+template <int NM_, int TX, int TY>
+Variant make_chain_variant() {
+  using C = ChainCfg<NM_, TX, TY>;
+  Variant v;
+  v.fn = sweep_fp64_chain_kernel<NM_, TX, TY>;
+  v.smem = C::smem_bytes();
+  v.entry_bytes = (size_t)C::ENT * sizeof(double);
+  v.tx = TX;
+  v.ty = TY;
+  v.nch = 1;
+  v.threads = C::NT;
+  v.pass = 32;
   return v;
 }
 
@@ -84,6 +104,7 @@ Variant make_mixed() {
   v.ty = C::TY;
   v.nch = 1;
   v.threads = C::NT;
+  v.pass = 32;
   return v;
 }
 
@@ -97,16 +118,31 @@ Variant pick_mixed(int nm) {
   }
 }
 
+template <int NM_>
+Variant pick_chain(int tile) {
+  return tile == 24 ? make_chain_variant<NM_, 2, 4>() : make_chain_variant<NM_, 4, 2>();
+}
+
 // precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves.
-// tile: 0 = the default shape, 42 or 24 (FP64 only).  na <= 128: the FP64
-// kernels sweep 64 angles per pass, the mixed ones 32.
-Variant pick_variant(int nm, int na, int precision, int tile = 0) {
+// tile: 0 = the default shape, 42 or 24 (FP64 only).  kernel (FP64 only):
+// 0 = the chained-wavefront kernel, 32 angles per pass; 1 = the staged
+// kernel, up to 64 angles per pass.  na <= 128; the mixed kernels sweep 32
+// angles per pass.
+Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0) {
   if (na > 128) return Variant();
   if (precision == 1 || precision == 2) {
     if (tile != 0) return Variant();
     return precision == 1 ? pick_mixed<MIX_F16>(nm) : pick_mixed<MIX_BF16>(nm);
   }
   if (precision != 0) return Variant();
+  if (kernel == 0) {
+    switch (nm) {
+      case 4: return pick_chain<4>(tile);
+      case 8: return pick_chain<8>(tile);
+      case 16: return pick_chain<16>(tile);
+      default: return Variant();
+    }
+  }
   const int nch = na > 32 ? 2 : 1;
   switch (nm) {
     case 4: return pick_nch<4>(nch, tile);
@@ -222,7 +258,7 @@ struct SweeperImpl {
 // once, the mixed ones 32.  Angles are independent in the sweep (each has its
 // own faces), so a larger na is swept in passes over consecutive angle
 // ranges whose contributions add up in vo.
-static int pass_angles(const SweeperImpl& S) { return S.var.mix ? 32 : 64; }
+static int pass_angles(const SweeperImpl& S) { return S.var.pass; }
 
 // Schedule, device task table and grid of one compiled tile shape.
 static int setup_plan(const SweeperImpl& S, const Variant& var, Schedule& sched, int& gp_block, int*& d_tasks,
@@ -252,12 +288,13 @@ static int setup_plan(const SweeperImpl& S, const Variant& var, Schedule& sched,
   return MSB_OK;
 }
 
-static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, int tile = 0, bool autotune = false) {
+static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, int tile = 0, bool autotune = false,
+                       int kernel = 0) {
   S.dims = dims;
   S.precision = precision;
   if (dims.ncell_x <= 0 || dims.ncell_y <= 0 || dims.ncell_z <= 0 || dims.ne <= 0 || dims.na <= 0)
     return set_error(MSB_ERR_ARG, "invalid dimensions");
-  S.var = pick_variant(dims.nm, dims.na, precision, tile);
+  S.var = pick_variant(dims.nm, dims.na, precision, tile, kernel);
   if (!S.var.valid())
     return set_error(MSB_ERR_UNSUPPORTED,
                      "no kernel variant for nm=%d na=%d precision=%d tile=%d (nm in {4,8,16}; na <= 128; "
@@ -274,7 +311,7 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
   long long ntask = S.sched.ntask();
   if (autotune) {
     S.autotune = true;
-    S.alt.var = pick_variant(dims.nm, dims.na, precision, S.var.tx == 4 ? 24 : 42);
+    S.alt.var = pick_variant(dims.nm, dims.na, precision, S.var.tx == 4 ? 24 : 42, kernel);
     if ((rc = setup_plan(S, S.alt.var, S.alt.sched, S.alt.gp_block, S.alt.d_tasks, S.alt.grid))) return rc;
     ntask = std::max(ntask, S.alt.sched.ntask());
   }
@@ -556,6 +593,9 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // 1: the first sweep times both FP64 tile shapes and keeps the faster
   const int autotune = Arguments_consume_int_or_default(args, "--autotune", 0);
   if (autotune != 0 && autotune != 1) return msb::set_error(MSB_ERR_ARG, "--autotune must be 0 or 1");
+  // FP64 sweep kernel: 0 = chained wavefront (default), 1 = the staged kernel
+  const int fp64_kernel = Arguments_consume_int_or_default(args, "--fp64_kernel", 0);
+  if (fp64_kernel != 0 && fp64_kernel != 1) return msb::set_error(MSB_ERR_ARG, "--fp64_kernel must be 0 or 1");
   // energy-group slice of a larger problem: group ie of the arrays is global
   // group ie_base + ie (one process per GPU, each sweeping its own groups)
   const int ie_base = Arguments_consume_int_or_default(args, "--ie_base", 0);
@@ -565,7 +605,7 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
   if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
   S->ie_base = ie_base;
-  const int rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0);
+  const int rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0, fp64_kernel);
   if (rc) return rc;
   sweeper->impl_ = S.release();
   return MSB_OK;

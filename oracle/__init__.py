@@ -34,6 +34,9 @@ def build(with_reference: bool | None = None) -> None:
         with_reference = os.path.isdir(os.path.join(reference_tree(), "src"))
     if with_reference:
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+        # the reference's own CUDA sweep for sm_100a (a timing comparator)
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref_cuda"], stdout=subprocess.DEVNULL,
+                              stderr=subprocess.DEVNULL)
         # the reference's driver programs linked with the product library
         if os.path.exists(os.path.join(os.path.dirname(HERE), "minisweep_b200", "libminisweep_b200.so")):
             subprocess.check_call(["make", "-s", "-C", HERE, "dropin"])

@@ -41,9 +41,9 @@ BUILTIN = [
     (4, 3, 5, 20, 32, 16),
     (5, 5, 5, 30, 33, 16),   # the reference's default flags
     (7, 6, 5, 4, 64, 16),
-    (6, 5, 4, 3, 100, 8),    # na > 64: passes of 64 angles, later passes add to vo
+    (6, 5, 4, 3, 100, 8),    # na > 32: passes over angle ranges, later passes add to vo
     (4, 4, 4, 2, 128, 16),
-    (3, 4, 5, 3, 65, 16),    # a one-angle second pass
+    (3, 4, 5, 3, 65, 16),    # a one-angle last pass
     (16, 16, 16, 16, 32, 4),  # the CPU-runnable headline case
 ]
 
@@ -57,6 +57,16 @@ def test_builtin_bitexact(nx, ny, nz, ne, na, nm):
     normsq, normsqdiff = oracle.norms(vi, vo)
     assert normsqdiff == 0.0
     assert normsq == oracle.normsq_closed_form(nx, ny, nz, ne, nm)
+
+
+@pytest.mark.parametrize("nx,ny,nz,ne,na,nm", [BUILTIN[i] for i in (0, 1, 2, 3, 7, 8, 9, 10, 11)])
+def test_builtin_bitexact_staged_kernel(nx, ny, nz, ne, na, nm):
+    # the staged FP64 kernel (--fp64_kernel 1; 64-angle passes), which the
+    # batched and the no-allocation sweeps also use
+    vi, vo = run_builtin(nx, ny, nz, ne, na, nm, "--fp64_kernel 1")
+    a, m = oracle.am_matrices(nm, na)
+    ref = oracle.sweep(nx, ny, nz, ne, nm, na, a, m, vi)
+    assert np.array_equal(vo, ref), f"max abs diff {np.max(np.abs(vo - ref))}"
 
 
 @pytest.mark.parametrize("extra", ["--nblock_z 2", "--nthread_octant 8 --nthread_e 4",
@@ -76,8 +86,10 @@ def test_builtin_flags_invariant(extra):
     (9, 7, 6, 5, 32, 4, "--tile 42"),
     (9, 7, 6, 5, 32, 16, "--autotune 1"),
     (6, 5, 4, 3, 40, 8, "--autotune 1 --tile 24"),
-    (5, 4, 3, 3, 128, 16, "--tile 24"),      # two 64-angle passes
-    (4, 5, 3, 2, 100, 4, "--autotune 1"),    # a 64-angle and a 36-angle pass
+    (5, 4, 3, 3, 128, 16, "--tile 24"),      # several angle passes
+    (4, 5, 3, 2, 100, 4, "--autotune 1"),    # a ragged last angle pass
+    (7, 6, 5, 4, 64, 16, "--tile 24 --fp64_kernel 1"),
+    (4, 5, 3, 2, 100, 4, "--autotune 1 --fp64_kernel 1"),
 ])
 def test_tile_shapes_bitexact(nx, ny, nz, ne, na, nm, extra):
     # the 2 x 4 tile (and the autotuned choice, whose first sweep runs both
@@ -108,10 +120,11 @@ RANDOM = [
 ]
 
 
+@pytest.mark.parametrize("kernel", [0, 1])
 @pytest.mark.parametrize("nx,ny,nz,ne,na,nm", RANDOM)
-def test_random_inputs(nx, ny, nz, ne, na, nm):
+def test_random_inputs(nx, ny, nz, ne, na, nm, kernel):
     a, m, vi = oracle.random_problem(nx, ny, nz, ne, nm, na, seed=1234)
-    with msb.Problem(flags(nx, ny, nz, ne, na), nm=nm) as pb:
+    with msb.Problem(flags(nx, ny, nz, ne, na, f"--fp64_kernel {kernel}"), nm=nm) as pb:
         pb.set_matrices(a, m)
         vo = pb.sweep_host(vi)
     ref = oracle.sweep(nx, ny, nz, ne, nm, na, a, m, vi)
