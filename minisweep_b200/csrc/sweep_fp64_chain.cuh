@@ -281,6 +281,15 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
     const size_t slab = (size_t)NM_ * NU * Q.nx * Q.ny;  // one (iz, ie) layer of the state
     const size_t zlayer = slab * Q.ne;
     const bool leader = warp == 0 && lane == 0;
+    // L2 policies (with Q.l2_hints): faces leaving a tile are kept
+    // (evict_last) until the downstream tile reads them; the state and the
+    // faces read are streamed (evict_first)
+    const bool hints = Q.l2_hints != 0;
+    const uint64_t pol_first = l2_policy_evict_first(), pol_last = l2_policy_evict_last();
+    auto cpa = [&](double* d, const double* src) {
+      if (hints) cp_async16_hint(d, src, pol_first);
+      else cp_async16(d, src);
+    };
 
     // leader state: assignment of start steps
     long long last_start = 0, last_end_all = 0;  // last task's start; step after every warp finished it
@@ -343,8 +352,8 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
               if (2 * gp + g2 >= Q.ne) continue;
 #pragma unroll
               for (int o = lane * 2; o < VSZ / 2; o += 64) {
-                cp_async16(dst + g2 * (VSZ / 2) + o, Q.vi + off0 + g2 * slab + o);
-                if (!pfirst) cp_async16(dst + VSZ + g2 * (VSZ / 2) + o, Q.vo + off0 + g2 * slab + o);
+                cpa(dst + g2 * (VSZ / 2) + o, Q.vi + off0 + g2 * slab + o);
+                if (!pfirst) cpa(dst + VSZ + g2 * (VSZ / 2) + o, Q.vo + off0 + g2 * slab + o);
               }
             }
             const size_t ez = (size_t)(oct * Q.ngp + gp) * Q.nz;
@@ -352,20 +361,20 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
               const double* src = Q.fyz + ((ez + piz) * Q.ny + piy) * (size_t)ENT;
               double* d2 = ringyz + (size_t)(wb * D + rs2) * ENT;
 #pragma unroll
-              for (int o = lane * 2; o < ENT; o += 64) cp_async16(d2 + o, src + o);
+              for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
             }
             if (wb == 0 && (fl & TF_Y_IN)) {
               const double* src = Q.fxz + ((ez + piz) * Q.nx + pix) * (size_t)ENT;
               double* d2 = ringxz + (size_t)(wa * D + rs2) * ENT;
 #pragma unroll
-              for (int o = lane * 2; o < ENT; o += 64) cp_async16(d2 + o, src + o);
+              for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
             }
             if (c2 == 0 && (fl & TF_Z_IN)) {
               const size_t ey = (size_t)(oct * Q.ngp + gp) * Q.ny;
               const double* src = Q.fxy + ((ey + piy) * Q.nx + pix) * (size_t)ENT;
               double* d2 = bufxy + (size_t)warp * ENT;
 #pragma unroll
-              for (int o = lane * 2; o < ENT; o += 64) cp_async16(d2 + o, src + o);
+              for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
             }
           }
         }
@@ -539,9 +548,15 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
             const double2 ov = make_double2(out[0], out[1]);
             *reinterpret_cast<double2*>(out_yz + eo) = ov;
             *reinterpret_cast<double2*>(out_xz + eo) = ov;
-            if (gout_yz) __stcg(reinterpret_cast<double2*>(gout_yz + eo), ov);
-            if (gout_xz) __stcg(reinterpret_cast<double2*>(gout_xz + eo), ov);
-            if (gout_xy) __stcg(reinterpret_cast<double2*>(gout_xy + eo), ov);
+            if (hints) {
+              if (gout_yz) st_v2_hint(gout_yz + eo, out[0], out[1], pol_last);
+              if (gout_xz) st_v2_hint(gout_xz + eo, out[0], out[1], pol_last);
+              if (gout_xy) st_v2_hint(gout_xy + eo, out[0], out[1], pol_last);
+            } else {
+              if (gout_yz) __stcg(reinterpret_cast<double2*>(gout_yz + eo), ov);
+              if (gout_xz) __stcg(reinterpret_cast<double2*>(gout_xz + eo), ov);
+              if (gout_xy) __stcg(reinterpret_cast<double2*>(gout_xy + eo), ov);
+            }
             // ---- angles -> moments for this t (psi is the B operand as is)
 #pragma unroll
             for (int i = 0; i < 2; ++i)
@@ -560,7 +575,9 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
                 if (8 * mt + q4 < NM_) {
                   const int o = NM_ * j + 8 * mt;
                   const double dsum = __dadd_rn(d2[mt][0][j], d2[mt][1][j]);
-                  vdst[o] = c_first ? dsum : __dadd_rn(vold[o], dsum);
+                  const double vnew = c_first ? dsum : __dadd_rn(vold[o], dsum);
+                  if (hints) st_f64_hint(vdst + o, vnew, pol_first);
+                  else vdst[o] = vnew;
                 }
               }
           }

@@ -61,6 +61,7 @@ struct Fp64Prob {
   int ia_base;  // angle index of the first angle of afm / mfa (a multiple of 64: passes over na > 64)
   int ie_base;  // global index of group 0 (energy-group slices of a larger problem)
   int vo_add;   // nonzero: every phase adds to vo (the passes after the first)
+  int l2_hints; // nonzero: faces written evict_last, state and consumed faces evict_first (chained kernel)
 };
 
 // One problem per launch.

@@ -237,6 +237,8 @@ struct SweeperImpl {
   AltPlan alt;
   float tune_ms[2] = {0.f, 0.f};  // first sweep: the chosen shape, the other shape
   int ie_base = 0;                // --ie_base: global index of this sweeper's group 0
+  int window = 4;                 // --task_window: tasks between a tile and its downwind neighbour, x SMs
+  int l2_hints = 0;               // --l2_hints: L2 eviction policies in the chained FP64 kernel
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
@@ -268,7 +270,7 @@ static int setup_plan(const SweeperImpl& S, const Variant& var, Schedule& sched,
   // a window of ~4 x SMs consecutive tasks between a tile and its downwind
   // neighbour in the table: measured on 64^3 x ne 64 (FP64 / mixed ms per
   // sweep) 131.5 / 99.7 with 1 x SMs, 124.5 / 91.1 with 2 x, 122.9 / 89.0 with 4 x
-  gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, var.tx, var.ty, 4 * S.nsm);
+  gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, var.tx, var.ty, S.window * S.nsm);
   if ((rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, var.tx, var.ty, gp_block, sched)))
     return rc;
   const long long ntask = sched.ntask();
@@ -382,6 +384,7 @@ static void fill_params(const SweeperImpl& S, X& x, PP& P, const double* vi_d, c
   x.ngp = S.ngp;
   x.ia_base = 0;
   x.ie_base = S.ie_base;
+  if constexpr (std::is_same<X, Fp64Prob>::value) x.l2_hints = S.l2_hints;
   P.tasks = d_tasks;
   P.ntask = ntask;
   P.sy.sync = S.d_sync;
@@ -394,7 +397,7 @@ static int launch_fp64(SweeperImpl& S, const Variant& var, const int* d_tasks, l
   const int na = S.dims.na, pa = pass_angles(S), npass = (na + pa - 1) / pa;
   int rc;
   for (int c = 0; c < npass; ++c) {
-    Fp64Params P;
+    Fp64Params P{};
     fill_params<double>(S, P.pr, P, vi_d, d_tasks, ntask);
     P.pr.vo = vo_d;
     P.pr.vo_add = c > 0 ? 1 : 0;  // later passes add to vo in every phase
@@ -596,6 +599,13 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // FP64 sweep kernel: 0 = chained wavefront (default), 1 = the staged kernel
   const int fp64_kernel = Arguments_consume_int_or_default(args, "--fp64_kernel", 0);
   if (fp64_kernel != 0 && fp64_kernel != 1) return msb::set_error(MSB_ERR_ARG, "--fp64_kernel must be 0 or 1");
+  // tasks between a tile and its downwind neighbour in the schedule, in
+  // multiples of the SM count
+  const int task_window = Arguments_consume_int_or_default(args, "--task_window", 4);
+  if (task_window < 1 || task_window > 64) return msb::set_error(MSB_ERR_ARG, "--task_window must be in [1, 64]");
+  // L2 eviction policies in the chained FP64 kernel: 1 = keep faces, stream the state
+  const int l2_hints = Arguments_consume_int_or_default(args, "--l2_hints", 0);
+  if (l2_hints != 0 && l2_hints != 1) return msb::set_error(MSB_ERR_ARG, "--l2_hints must be 0 or 1");
   // energy-group slice of a larger problem: group ie of the arrays is global
   // group ie_base + ie (one process per GPU, each sweeping its own groups)
   const int ie_base = Arguments_consume_int_or_default(args, "--ie_base", 0);
@@ -605,6 +615,8 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
   if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
   S->ie_base = ie_base;
+  S->window = task_window;
+  S->l2_hints = l2_hints;
   const int rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0, fp64_kernel);
   if (rc) return rc;
   sweeper->impl_ = S.release();
