@@ -338,10 +338,18 @@ int msb_initialize_state_slice_device(double* v_d, Dimensions dims, int ie_base,
 /* Kernel statistics of the last sweep: number of tasks, kernel launches. */
 int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int* nlaunch);
 /* Tile shape (cell columns per CTA) the sweeper uses and, with --autotune 1,
- * the first sweep's times (ms) of the chosen and the other shape (0 before
- * that sweep, or without autotuning).  No reference counterpart: the
- * reference's --ncell_{x,y}_per_subblock size its CPU/GPU thread blocks. */
+ * the first sweep's times (ms) of the chosen plan and of the fastest plan
+ * with the other tile shape (0 before that sweep, or without autotuning).
+ * No reference counterpart: the reference's --ncell_{x,y}_per_subblock size
+ * its CPU/GPU thread blocks. */
 int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_chosen, float* ms_other);
+/* The rest of the FP64 plan in use: the task window (x SMs) of its schedule,
+ * the L2 policy flag, and how many plans --autotune 1 timed (1 without it).
+ * With --autotune 1 the first sweep runs every candidate -- both tile shapes,
+ * task windows 2, 4 and 8, and for the chained kernel both L2 policies --
+ * and keeps the fastest.  No reference counterpart (the reference's tuning
+ * flags, sweeper_kba_c.h:54-233, are set by hand). */
+int Sweeper_plan(const Sweeper* sweeper, int* task_window, int* l2_hints, int* ncandidates);
 /* Copy of the schedule (one record of MSB_TASK_INTS ints per task, in launch
  * order) for host-side checks; returns the task count, or <0. */
 enum { MSB_TASK_INTS = 16 };

@@ -197,13 +197,17 @@ int encode_state_map(CUtensorMap* map, const double* ptr, const Dimensions& d, i
 
 }  // namespace
 
-// The other FP64 tile shape of an autotuning sweeper, with its own schedule.
+// One way to sweep an FP64 problem that --autotune 1 tries: a compiled kernel
+// (tile shape), the schedule built for a task window, and the L2 policy.
 struct AltPlan {
   Variant var;
   Schedule sched;
   int gp_block = 1;
   int* d_tasks = nullptr;
   int grid = 0;
+  int window = 4;
+  int l2_hints = 0;
+  float ms = 0.f;  // its autotuning sweep
 };
 
 struct SweeperImpl {
@@ -231,18 +235,19 @@ struct SweeperImpl {
   int nlaunch = 0;
   int nsm = 0;
   int* h_status = nullptr;  // pinned copy of the status words
-  // --autotune 1: the first sweep runs with both tile shapes and keeps the faster
+  // --autotune 1: the first sweep runs with every candidate plan (tile shape
+  // x task window x L2 policy) and keeps the fastest
   bool autotune = false;
   bool tuned = false;
-  AltPlan alt;
-  float tune_ms[2] = {0.f, 0.f};  // first sweep: the chosen shape, the other shape
+  std::vector<AltPlan> alts;
+  float tune_ms[2] = {0.f, 0.f};  // first sweep: the chosen plan, the fastest of the other tile shape
   int ie_base = 0;                // --ie_base: global index of this sweeper's group 0
   int window = 4;                 // --task_window: tasks between a tile and its downwind neighbour, x SMs
   int l2_hints = 0;               // --l2_hints: L2 eviction policies in the chained FP64 kernel
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
-    cudaFree(alt.d_tasks);
+    for (auto& a : alts) cudaFree(a.d_tasks);
     cudaFree(d_sync);
     for (auto& f : d_face) cudaFree(f);
     cudaFree(d_afm);
@@ -262,15 +267,14 @@ struct SweeperImpl {
 // ranges whose contributions add up in vo.
 static int pass_angles(const SweeperImpl& S) { return S.var.pass; }
 
-// Schedule, device task table and grid of one compiled tile shape.
-static int setup_plan(const SweeperImpl& S, const Variant& var, Schedule& sched, int& gp_block, int*& d_tasks,
-                      int& grid) {
+// Schedule, device task table and grid of one compiled tile shape, with a
+// window of `window` x SMs consecutive tasks between a tile and its downwind
+// neighbour in the table.
+static int setup_plan(const SweeperImpl& S, const Variant& var, int window, Schedule& sched, int& gp_block,
+                      int*& d_tasks, int& grid) {
   const Dimensions& dims = S.dims;
   int rc, occ = 0;
-  // a window of ~4 x SMs consecutive tasks between a tile and its downwind
-  // neighbour in the table: measured on 64^3 x ne 64 (FP64 / mixed ms per
-  // sweep) 131.5 / 99.7 with 1 x SMs, 124.5 / 91.1 with 2 x, 122.9 / 89.0 with 4 x
-  gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, var.tx, var.ty, S.window * S.nsm);
+  gp_block = pick_gp_block(dims.ncell_x, dims.ncell_y, S.ngp, var.tx, var.ty, window * S.nsm);
   if ((rc = build_schedule(dims.ncell_x, dims.ncell_y, dims.ncell_z, S.ngp, var.tx, var.ty, gp_block, sched)))
     return rc;
   const long long ntask = sched.ntask();
@@ -309,13 +313,31 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
   if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
   if ((rc = cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rc;
   S.nsm = nsm;
-  if ((rc = setup_plan(S, S.var, S.sched, S.gp_block, S.d_tasks, S.grid))) return rc;
+  if ((rc = setup_plan(S, S.var, S.window, S.sched, S.gp_block, S.d_tasks, S.grid))) return rc;
   long long ntask = S.sched.ntask();
   if (autotune) {
+    // candidates: both tile shapes x task windows of 2, 4 and 8 x SMs (x both
+    // L2 policies for the chained kernel), besides the sweeper's own plan
     S.autotune = true;
-    S.alt.var = pick_variant(dims.nm, dims.na, precision, S.var.tx == 4 ? 24 : 42, kernel);
-    if ((rc = setup_plan(S, S.alt.var, S.alt.sched, S.alt.gp_block, S.alt.d_tasks, S.alt.grid))) return rc;
-    ntask = std::max(ntask, S.alt.sched.ntask());
+    const int windows[3] = {2, 4, 8};
+    const int nh = kernel == 0 ? 2 : 1;
+    for (int t = 0; t < 2; ++t)
+      for (int w : windows)
+        for (int h = 0; h < nh; ++h) {
+          const int tile_c = t == 0 ? 42 : 24;
+          const bool is_main = (S.var.tx == 4) == (t == 0) && w == S.window && (nh == 1 || h == S.l2_hints);
+          if (is_main) continue;
+          AltPlan a;
+          a.var = pick_variant(dims.nm, dims.na, precision, tile_c, kernel);
+          a.window = w;
+          a.l2_hints = nh == 1 ? S.l2_hints : h;
+          if ((rc = setup_plan(S, a.var, a.window, a.sched, a.gp_block, a.d_tasks, a.grid))) {
+            cudaFree(a.d_tasks);
+            return rc;
+          }
+          ntask = std::max(ntask, a.sched.ntask());
+          S.alts.push_back(std::move(a));
+        }
   }
   S.sync_ints = SY_PROGRESS + (size_t)ntask;
   if ((rc = cuda_check(cudaMalloc(&S.d_sync, S.sync_ints * sizeof(int)), "cudaMalloc sync"))) return rc;
@@ -444,6 +466,19 @@ static int launch_mixed(SweeperImpl& S, double* vo_d, const double* vi_d, cudaSt
   return MSB_OK;
 }
 
+// Exchanges the sweeper's plan with a candidate.
+static void swap_plan(SweeperImpl& S, AltPlan& a) {
+  std::swap(S.var, a.var);
+  std::swap(S.sched, a.sched);
+  std::swap(S.gp_block, a.gp_block);
+  std::swap(S.d_tasks, a.d_tasks);
+  std::swap(S.grid, a.grid);
+  std::swap(S.window, a.window);
+  std::swap(S.l2_hints, a.l2_hints);
+}
+
+static int impl_sync(SweeperImpl& S, cudaStream_t stream);
+
 // Launches one sweep: vo_d = sweep(vi_d), asynchronously on `stream` (the
 // first sweep of an autotuning sweeper waits for the stream).
 static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
@@ -467,39 +502,56 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
   }
   if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
   if (S.var.fn && S.autotune && !S.tuned) {
-    // First sweep of an autotuning sweeper: the same sweep with each tile
-    // shape (each writes all of vo), timed on the stream; the faster shape
-    // is kept for every later sweep.
+    // First sweep of an autotuning sweeper: the same sweep with the sweeper's
+    // own plan and with every candidate (each writes all of vo), timed on the
+    // stream; the fastest plan is kept for every later sweep.
     S.tuned = true;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    for (auto& e : ev)
-      if ((rc = cuda_check(cudaEventCreate(&e), "autotune event"))) return rc;
-    cudaEventRecord(ev[0], stream);
-    rc = launch_fp64(S, S.var, S.d_tasks, S.sched.ntask(), S.grid, vo_d, vi_d, stream);
-    if (!rc) rc = cuda_check(cudaEventRecord(ev[1], stream), "autotune event");
-    if (!rc) rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
-                             "status copy");
-    if (!rc) rc = cuda_check(cudaStreamSynchronize(stream), "autotune sweep");
-    if (!rc && S.h_status[SY_ERROR] == 0) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if ((rc = cuda_check(cudaEventCreate(&e0), "autotune event"))) return rc;
+    if ((rc = cuda_check(cudaEventCreate(&e1), "autotune event"))) {
+      cudaEventDestroy(e0);
+      return rc;
+    }
+    float main_ms = 0.f;
+    // i = -1: the sweeper's own plan; i >= 0: candidate i (swapped in)
+    for (int i = -1; i < (int)S.alts.size() && !rc; ++i) {
+      if (i >= 0) swap_plan(S, S.alts[i]);
       rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync");
-      if (!rc) rc = launch_fp64(S, S.alt.var, S.alt.d_tasks, S.alt.sched.ntask(), S.alt.grid, vo_d, vi_d, stream);
-      if (!rc) rc = cuda_check(cudaEventRecord(ev[2], stream), "autotune event");
-      if (!rc) rc = cuda_check(cudaEventSynchronize(ev[2]), "autotune sweep");
-      if (!rc) {
-        cudaEventElapsedTime(&S.tune_ms[0], ev[0], ev[1]);
-        cudaEventElapsedTime(&S.tune_ms[1], ev[1], ev[2]);
-        if (S.tune_ms[1] < S.tune_ms[0]) {
-          std::swap(S.var, S.alt.var);
-          std::swap(S.sched, S.alt.sched);
-          std::swap(S.gp_block, S.alt.gp_block);
-          std::swap(S.d_tasks, S.alt.d_tasks);
-          std::swap(S.grid, S.alt.grid);
-          std::swap(S.tune_ms[0], S.tune_ms[1]);
-        }
+      if (!rc) rc = cuda_check(cudaEventRecord(e0, stream), "autotune event");
+      if (!rc) rc = launch_fp64(S, S.var, S.d_tasks, S.sched.ntask(), S.grid, vo_d, vi_d, stream);
+      if (!rc) rc = cuda_check(cudaEventRecord(e1, stream), "autotune event");
+      if (!rc) rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
+                               "status copy");
+      if (!rc) rc = cuda_check(cudaStreamSynchronize(stream), "autotune sweep");
+      float ms = 0.f;
+      if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+      if (!rc && S.h_status[SY_ERROR] != 0) rc = impl_sync(S, stream);  // reports the device error
+      if (i >= 0) {
+        swap_plan(S, S.alts[i]);
+        S.alts[i].ms = ms;
+      } else {
+        main_ms = ms;
       }
     }
-    for (auto& e : ev) cudaEventDestroy(e);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     if (rc) return rc;
+    int best = -1;
+    float best_ms = main_ms;
+    for (int i = 0; i < (int)S.alts.size(); ++i)
+      if (S.alts[i].ms < best_ms) {
+        best = i;
+        best_ms = S.alts[i].ms;
+      }
+    if (best >= 0) {
+      swap_plan(S, S.alts[best]);
+      S.alts[best].ms = main_ms;  // the slot now holds the former main plan
+    }
+    S.tune_ms[0] = best_ms;
+    S.tune_ms[1] = 0.f;
+    for (const auto& a : S.alts)
+      if (a.var.tx != S.var.tx && (S.tune_ms[1] == 0.f || a.ms < S.tune_ms[1])) S.tune_ms[1] = a.ms;
+    // the sync words hold the last trial's status, which was clean
   } else if (S.var.fn) {
     if ((rc = launch_fp64(S, S.var, S.d_tasks, S.sched.ntask(), S.grid, vo_d, vi_d, stream))) return rc;
   } else {
@@ -694,6 +746,15 @@ extern "C" int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_
   if (ty) *ty = S->var.ty;
   if (ms_chosen) *ms_chosen = S->tuned ? S->tune_ms[0] : 0.f;
   if (ms_other) *ms_other = S->tuned ? S->tune_ms[1] : 0.f;
+  return MSB_OK;
+}
+
+extern "C" int Sweeper_plan(const Sweeper* sweeper, int* task_window, int* l2_hints, int* ncandidates) {
+  const SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  if (task_window) *task_window = S->window;
+  if (l2_hints) *l2_hints = S->l2_hints;
+  if (ncandidates) *ncandidates = S->autotune ? 1 + (int)S->alts.size() : 1;
   return MSB_OK;
 }
 
