@@ -34,6 +34,7 @@ struct Variant {
   size_t entry_bytes = 0;  // one face entry (octant, group pair, position)
   int tx = 0, ty = 0, nch = 0, threads = 0;
   int pass = 64;  // angles swept per launch (na above it is swept in passes)
+  int kernel = 0; // FP64: 0 staged, 1 chained wavefront
   bool valid() const { return fn || mix; }
   const void* func() const { return fn ? (const void*)fn : (const void*)mix; }
 };
@@ -74,6 +75,7 @@ Variant make_chain_variant() {
   v.nch = 1;
   v.threads = C::NT;
   v.pass = 32;
+  v.kernel = 1;
   return v;
 }
 
@@ -125,9 +127,9 @@ Variant pick_chain(int tile) {
 
 // precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves.
 // tile: 0 = the default shape, 42 or 24 (FP64 only).  kernel (FP64 only):
-// 0 = the chained-wavefront kernel, 32 angles per pass; 1 = the staged
-// kernel, up to 64 angles per pass.  na <= 128; the mixed kernels sweep 32
-// angles per pass.
+// 0 = the staged kernel, up to 64 angles per pass; 1 = the chained-wavefront
+// kernel, 32 angles per pass.  na <= 128; the mixed kernels sweep 32 angles
+// per pass.
 Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0) {
   if (na > 128) return Variant();
   if (precision == 1 || precision == 2) {
@@ -135,7 +137,7 @@ Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0
     return precision == 1 ? pick_mixed<MIX_F16>(nm) : pick_mixed<MIX_BF16>(nm);
   }
   if (precision != 0) return Variant();
-  if (kernel == 0) {
+  if (kernel == 1) {
     switch (nm) {
       case 4: return pick_chain<4>(tile);
       case 8: return pick_chain<8>(tile);
@@ -316,21 +318,20 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
   if ((rc = setup_plan(S, S.var, S.window, S.sched, S.gp_block, S.d_tasks, S.grid))) return rc;
   long long ntask = S.sched.ntask();
   if (autotune) {
-    // candidates: both tile shapes x task windows of 2, 4 and 8 x SMs (x both
-    // L2 policies for the chained kernel), besides the sweeper's own plan
+    // candidates: both FP64 kernels x both tile shapes x task windows of 4,
+    // 8 and 16 x SMs, besides the sweeper's own plan
     S.autotune = true;
-    const int windows[3] = {2, 4, 8};
-    const int nh = kernel == 0 ? 2 : 1;
-    for (int t = 0; t < 2; ++t)
-      for (int w : windows)
-        for (int h = 0; h < nh; ++h) {
+    const int windows[3] = {4, 8, 16};
+    for (int k = 0; k < 2; ++k)
+      for (int t = 0; t < 2; ++t)
+        for (int w : windows) {
           const int tile_c = t == 0 ? 42 : 24;
-          const bool is_main = (S.var.tx == 4) == (t == 0) && w == S.window && (nh == 1 || h == S.l2_hints);
+          const bool is_main = k == kernel && (S.var.tx == 4) == (t == 0) && w == S.window;
           if (is_main) continue;
           AltPlan a;
-          a.var = pick_variant(dims.nm, dims.na, precision, tile_c, kernel);
+          a.var = pick_variant(dims.nm, dims.na, precision, tile_c, k);
           a.window = w;
-          a.l2_hints = nh == 1 ? S.l2_hints : h;
+          a.l2_hints = S.l2_hints;
           if ((rc = setup_plan(S, a.var, a.window, a.sched, a.gp_block, a.d_tasks, a.grid))) {
             cudaFree(a.d_tasks);
             return rc;
@@ -339,11 +340,19 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
           S.alts.push_back(std::move(a));
         }
   }
+  // face entries and angle passes of every plan the sweeper may run
+  size_t entry_bytes = S.var.entry_bytes;
+  int pass_min = S.var.pass, pass_max = S.var.pass;
+  for (const auto& a : S.alts) {
+    entry_bytes = std::max(entry_bytes, a.var.entry_bytes);
+    pass_min = std::min(pass_min, a.var.pass);
+    pass_max = std::max(pass_max, a.var.pass);
+  }
   S.sync_ints = SY_PROGRESS + (size_t)ntask;
   if ((rc = cuda_check(cudaMalloc(&S.d_sync, S.sync_ints * sizeof(int)), "cudaMalloc sync"))) return rc;
   if ((rc = cuda_check(cudaMallocHost(&S.h_status, 8 * sizeof(int)), "cudaMallocHost status"))) return rc;
 
-  const size_t per = (size_t)NOCTANT * S.ngp * S.var.entry_bytes;
+  const size_t per = (size_t)NOCTANT * S.ngp * entry_bytes;
   S.face_bytes[0] = per * dims.ncell_y * dims.ncell_x;
   S.face_bytes[1] = per * dims.ncell_z * dims.ncell_x;
   S.face_bytes[2] = per * dims.ncell_z * dims.ncell_y;
@@ -357,8 +366,8 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
   const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
   if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
   if ((rc = cuda_check(cudaMalloc(&S.d_mfa, nmat * sizeof(double)), "cudaMalloc m_from_a"))) return rc;
-  if (dims.na > pass_angles(S)) {
-    const size_t npass_mat = (size_t)dims.nm * pass_angles(S) * NOCTANT;
+  if (dims.na > pass_min) {
+    const size_t npass_mat = (size_t)dims.nm * pass_max * NOCTANT;
     if ((rc = cuda_check(cudaMalloc(&S.d_afm_c, npass_mat * sizeof(double)), "cudaMalloc a_from_m pass"))) return rc;
     if ((rc = cuda_check(cudaMalloc(&S.d_mfa_c, npass_mat * sizeof(double)), "cudaMalloc m_from_a pass"))) return rc;
   }
@@ -648,7 +657,7 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // 1: the first sweep times both FP64 tile shapes and keeps the faster
   const int autotune = Arguments_consume_int_or_default(args, "--autotune", 0);
   if (autotune != 0 && autotune != 1) return msb::set_error(MSB_ERR_ARG, "--autotune must be 0 or 1");
-  // FP64 sweep kernel: 0 = chained wavefront (default), 1 = the staged kernel
+  // FP64 sweep kernel: 0 = the staged kernel (default), 1 = the chained wavefront
   const int fp64_kernel = Arguments_consume_int_or_default(args, "--fp64_kernel", 0);
   if (fp64_kernel != 0 && fp64_kernel != 1) return msb::set_error(MSB_ERR_ARG, "--fp64_kernel must be 0 or 1");
   // tasks between a tile and its downwind neighbour in the schedule, in
@@ -749,9 +758,11 @@ extern "C" int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_
   return MSB_OK;
 }
 
-extern "C" int Sweeper_plan(const Sweeper* sweeper, int* task_window, int* l2_hints, int* ncandidates) {
+extern "C" int Sweeper_plan(const Sweeper* sweeper, int* fp64_kernel, int* task_window, int* l2_hints,
+                            int* ncandidates) {
   const SweeperImpl* S = impl_of(sweeper);
   if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  if (fp64_kernel) *fp64_kernel = S->var.kernel;
   if (task_window) *task_window = S->window;
   if (l2_hints) *l2_hints = S->l2_hints;
   if (ncandidates) *ncandidates = S->autotune ? 1 + (int)S->alts.size() : 1;

@@ -59,10 +59,9 @@ def test_builtin_bitexact(nx, ny, nz, ne, na, nm):
     assert normsq == oracle.normsq_closed_form(nx, ny, nz, ne, nm)
 
 
-@pytest.mark.parametrize("nx,ny,nz,ne,na,nm", [BUILTIN[i] for i in (0, 1, 2, 3, 7, 8, 9, 10, 11)])
-def test_builtin_bitexact_staged_kernel(nx, ny, nz, ne, na, nm):
-    # the staged FP64 kernel (--fp64_kernel 1; 64-angle passes), which the
-    # batched and the no-allocation sweeps also use
+@pytest.mark.parametrize("nx,ny,nz,ne,na,nm", BUILTIN)
+def test_builtin_bitexact_chained_kernel(nx, ny, nz, ne, na, nm):
+    # the chained-wavefront FP64 kernel (--fp64_kernel 1; 32-angle passes)
     vi, vo = run_builtin(nx, ny, nz, ne, na, nm, "--fp64_kernel 1")
     a, m = oracle.am_matrices(nm, na)
     ref = oracle.sweep(nx, ny, nz, ne, nm, na, a, m, vi)
