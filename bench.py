@@ -574,9 +574,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     IE_BASE = NE * rank
     flags = (f"--ncell_x {NX} --ncell_y {NY} --ncell_z {NZ} --ne {NE} --na {NA} --nblock_z {NBLOCK_Z} "
              f"--niterations {NITER} --ie_base {IE_BASE}")
-    # --autotune 1: the first (warm-up) sweep times both FP64 tile shapes and
-    # keeps the faster for every later sweep
-    pb = msb.Problem(flags + " --autotune 1", nm=NM)
+    # --autotune 1: the first (warm-up) sweep times every candidate plan
+    # (both FP64 kernels x both tile shapes x task windows) and keeps the
+    # fastest for every later sweep; --fp64-flags fixes the plan instead
+    pb = msb.Problem(flags + " " + (args.fp64_flags or "--autotune 1"), nm=NM)
     n = pb.nstate
     va = torch.empty(n, dtype=torch.float64, device=dev)
     vb = torch.empty(n, dtype=torch.float64, device=dev)
@@ -623,7 +624,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
 
     # correctness of the timed result (built-in Quantities: vo == vi exactly)
     normsq, normsqdiff = sum_norms(*pb.norms_device(va.data_ptr(), vb.data_ptr()))
-    mixed = measure_mixed(args, pb, flags, va, vb, stream, dev, world, ms_fp64=None)
+    mixed = [] if args.no_mixed else measure_mixed(args, pb, flags, va, vb, stream, dev, world, ms_fp64=None)
     closed = None
     try:
         import oracle
@@ -679,7 +680,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                                    f"{NE * world}-group problem; checksums all-reduced (2 FP64 scalars), no other "
                                    "exchange",
                     "tile": {"cells_per_cta": [tile["tx"], tile["ty"]],
-                             "autotune_first_sweep_ms": {"chosen": tile["ms_chosen"], "other": tile["ms_other"]}},
+                             "autotune_first_sweep_ms": {"chosen": tile["ms_chosen"],
+                                                         "best_other_tile": tile["ms_other"]}},
+                    "plan": {"fp64_kernel": "chained wavefront" if tile["fp64_kernel"] else "staged",
+                             "task_window_x_sms": tile["task_window"], "l2_hints": tile["l2_hints"],
+                             "plans_timed": tile["candidates"]},
                     "roofline": roofline, "cpu_baseline": cpu,
                     "e2e": e2e,
                     "clocks": clk, "gpu_launches": args.steps * NITER,
@@ -735,6 +740,9 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched serving workload")
     ap.add_argument("--no-dense", action="store_true", help="skip the 32x32x96 / ne 128 / na 128 case")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision sweeps")
+    ap.add_argument("--fp64-flags", default="", help="sweeper flags of the FP64 step instead of --autotune 1 "
+                                                     "(e.g. '--fp64_kernel 1 --tile 42 --task_window 8')")
     ap.add_argument("--batch-steps", type=int, default=2, help="timed batched sweeps")
     ap.add_argument("--batch-warmup", type=int, default=1, help="untimed batched sweeps")
     ap.add_argument("--case", choices=["config2", "small"], default="config2",
