@@ -300,12 +300,44 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
     int nknown = 0;  // tasks with an assigned start (from the shared counter)
     long long stop_step = -1;
     int kc = 0, kp = 0;  // compute / prefetch cursor (task index)
-    int kp_acq = -1;
-    bool have = false;  // task kc's constants are in registers
 
-    // task constants of the compute cursor
+    // prefetch cursor: constants of task kp for this warp (valid when p_have)
+    bool p_have = false, p_act = false, p_vo = false, p_g1 = false;
+    long long p_lo = 0, p_hi = 0;  // the warp's first step of the task, first step after it
+    long long p_off = 0, p_zs = 0;  // state offset (doubles) of plane 0 and per plane
+    int p_dz = 1;
+    const double* p_fyz = nullptr;  // faces entering at this warp's edges, plane 0
+    const double* p_fxz = nullptr;
+    const double* p_fxy = nullptr;
+    auto load_prefetch = [&]() {
+      mbar_test_wait(&sfull[kp % NSLOT], (uint32_t)((kp / NSLOT) & 1));  // acquire the loader's writes
+      const ChainDesc& dd = desc[kp % NSLOT];
+      const int oct = dd.rec[TK_OCT], gp = dd.rec[TK_GP], fl = dd.rec[TK_FLAGS];
+      const int w = dd.rec[TK_X1] - dd.rec[TK_X0], h = dd.rec[TK_Y1] - dd.rec[TK_Y0];
+      const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1;
+      p_dz = (oct & 4) ? -1 : 1;
+      p_lo = dd.start + wa + wb;
+      p_hi = p_lo + (dd.rec[TK_Z1] - dd.rec[TK_Z0]);
+      p_act = wa < w && wb < h;
+      p_vo = !((fl & TF_FIRST) != 0 && !Q.vo_add);
+      p_g1 = 2 * gp + 1 < Q.ne;
+      const int pix = dx > 0 ? dd.rec[TK_X0] + wa : dd.rec[TK_X1] - 1 - wa;
+      const int piy = dy > 0 ? dd.rec[TK_Y0] + wb : dd.rec[TK_Y1] - 1 - wb;
+      const int piz0 = p_dz > 0 ? dd.rec[TK_Z0] : dd.rec[TK_Z1] - 1;
+      p_off = (long long)((size_t)NM_ * NU * (pix + (size_t)Q.nx * piy) + slab * (size_t)(2 * gp) +
+                          zlayer * (size_t)piz0);
+      p_zs = p_dz * (long long)zlayer;
+      const size_t eo = (size_t)(oct * Q.ngp + gp);
+      p_fyz = (wa == 0 && (fl & TF_X_IN)) ? Q.fyz + ((eo * Q.nz + piz0) * Q.ny + piy) * (size_t)ENT : nullptr;
+      p_fxz = (wb == 0 && (fl & TF_Y_IN)) ? Q.fxz + ((eo * Q.nz + piz0) * Q.nx + pix) * (size_t)ENT : nullptr;
+      p_fxy = (fl & TF_Z_IN) ? Q.fxy + ((eo * Q.ny + piy) * Q.nx + pix) * (size_t)ENT : nullptr;
+      p_have = true;
+    };
+
+    // compute cursor: constants of task kc (valid when have)
+    bool have = false;
+    long long c_lo = 0, c_hi = 0;  // the warp's first step of the task, first step after it
     int c_oct = 0, c_gp = 0, c_flags = 0, c_nzr = 0, c_dz = 1, c_iz0 = 0;
-    long long c_start = 0;
     bool c_act = false, c_first = false, c_gval = false, c_gvo = false;
     bool x_in = false, y_in = false, z_in = false, x_out = false, y_out = false, z_out = false;
     int ix = 0, iy = 0, sp_xy = 0, g_vo = 0, gx = 0, gy = 0, gz = 0;
@@ -314,6 +346,59 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
     double b1r[KS][4];
     double a2r[MT][4][2];
     double carry[4][2];
+    // task kc's constants and matrices into registers (the previous task of
+    // this warp is finished, so its matrices are free)
+    auto load_compute = [&]() {
+      const int qs = kc % NSLOT;
+      mbar_test_wait(&sfull[qs], (uint32_t)((kc / NSLOT) & 1));  // acquire the loader's writes
+      const ChainDesc& dd = desc[qs];
+      c_oct = dd.rec[TK_OCT];
+      c_gp = dd.rec[TK_GP];
+      c_flags = dd.rec[TK_FLAGS];
+      c_nzr = dd.rec[TK_Z1] - dd.rec[TK_Z0];
+      c_lo = dd.start + wa + wb;
+      c_hi = c_lo + c_nzr;
+      const int w = dd.rec[TK_X1] - dd.rec[TK_X0], h = dd.rec[TK_Y1] - dd.rec[TK_Y0];
+      const int dx = (c_oct & 1) ? -1 : 1, dy = (c_oct & 2) ? -1 : 1;
+      c_dz = (c_oct & 4) ? -1 : 1;
+      c_act = wa < w && wb < h;
+      c_first = (c_flags & TF_FIRST) != 0 && !Q.vo_add;
+      ix = dx > 0 ? dd.rec[TK_X0] + wa : dd.rec[TK_X1] - 1 - wa;
+      iy = dy > 0 ? dd.rec[TK_Y0] + wb : dd.rec[TK_Y1] - 1 - wb;
+      c_iz0 = c_dz > 0 ? dd.rec[TK_Z0] : dd.rec[TK_Z1] - 1;
+      const int g_col = 2 * c_gp + (q4 >> 2);
+      c_gval = g_col < Q.ne;
+      g_vo = 2 * c_gp + (r >> 1);
+      c_gvo = g_vo < Q.ne;
+      so = (double)(1 + c_oct);
+      so_r = 1.0 / so;  // rounded, as the reference's 1/(1+octant)
+      face_k = c_gval ? (double)d_scale_energy(Q.ie_base + g_col) * (double)d_scale_unknown(q4 & 3) * so : 0.0;
+      sp_xy = ix + 3 * iy + 2;
+      col = (size_t)NM_ * NU * (ix + (size_t)Q.nx * iy);
+      ent_z = (size_t)(c_oct * Q.ngp + c_gp) * Q.nz;
+      ent_y = (size_t)(c_oct * Q.ngp + c_gp) * Q.ny;
+      x_in = wa == 0 && (c_flags & TF_X_IN);
+      y_in = wb == 0 && (c_flags & TF_Y_IN);
+      z_in = (c_flags & TF_Z_IN) != 0;
+      x_out = wa == w - 1 && (c_flags & TF_X_OUT);
+      y_out = wb == h - 1 && (c_flags & TF_Y_OUT);
+      z_out = (c_flags & TF_Z_OUT) != 0;
+      gx = dx > 0 ? -1 : Q.nx;
+      gy = dy > 0 ? -1 : Q.ny;
+      gz = c_dz > 0 ? -1 : Q.nz;
+      const double* mat = mats + qs * C::MAT;
+#pragma unroll
+      for (int k = 0; k < KS; ++k)
+#pragma unroll
+        for (int t = 0; t < 4; ++t) b1r[k][t] = mat[(k * 4 + t) * 32 + lane];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) a2r[mt][t][i] = mat[KS * 4 * 32 + ((mt * 4 + t) * 2 + i) * 32 + lane];
+      have = true;
+    };
 
     long long G = 0;
     int rs = 0;  // G % D
@@ -324,127 +409,68 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
         const long long G2 = G + LA;
         int rs2 = rs + LA;
         if (rs2 >= D) rs2 -= D;
-        while (kp < nknown) {
-          const ChainDesc& dd = desc[kp % NSLOT];
-          if (G2 < dd.start + wa + wb + (dd.rec[TK_Z1] - dd.rec[TK_Z0])) break;
-          ++kp;
-        }
-        if (kp < nknown) {
-          if (kp != kp_acq) {  // acquire the loader's writes of this slot
-            mbar_test_wait(&sfull[kp % NSLOT], (uint32_t)((kp / NSLOT) & 1));
-            kp_acq = kp;
+        for (;;) {
+          if (p_have && G2 >= p_hi) {
+            ++kp;
+            p_have = false;
+          } else if (!p_have && kp < nknown) {
+            load_prefetch();
+          } else {
+            break;
           }
-          const ChainDesc& dd = desc[kp % NSLOT];
-          const long long c2l = G2 - dd.start - wa - wb;
-          const int w = dd.rec[TK_X1] - dd.rec[TK_X0], h = dd.rec[TK_Y1] - dd.rec[TK_Y0];
-          if (c2l >= 0 && wa < w && wb < h) {
-            const int c2 = (int)c2l, oct = dd.rec[TK_OCT], gp = dd.rec[TK_GP], fl = dd.rec[TK_FLAGS];
-            const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
-            const int pix = dx > 0 ? dd.rec[TK_X0] + wa : dd.rec[TK_X1] - 1 - wa;
-            const int piy = dy > 0 ? dd.rec[TK_Y0] + wb : dd.rec[TK_Y1] - 1 - wb;
-            const int piz = (dz > 0 ? dd.rec[TK_Z0] : dd.rec[TK_Z1] - 1) + dz * c2;
-            const bool pfirst = (fl & TF_FIRST) != 0 && !Q.vo_add;
-            const size_t off0 = (size_t)NM_ * NU * (pix + (size_t)Q.nx * piy) + slab * (size_t)(2 * gp) +
-                                zlayer * (size_t)piz;
-            double* dst = ringv + (size_t)(warp * D + rs2) * 2 * VSZ;
+        }
+        if (p_have && p_act && G2 >= p_lo) {
+          const int c2 = (int)(G2 - p_lo);
+          const long long off0 = p_off + p_zs * c2;
+          double* dst = ringv + (size_t)(warp * D + rs2) * 2 * VSZ;
 #pragma unroll
-            for (int g2 = 0; g2 < 2; ++g2) {
-              if (2 * gp + g2 >= Q.ne) continue;
+          for (int g2 = 0; g2 < 2; ++g2) {
+            if (g2 == 1 && !p_g1) continue;
 #pragma unroll
-              for (int o = lane * 2; o < VSZ / 2; o += 64) {
-                cpa(dst + g2 * (VSZ / 2) + o, Q.vi + off0 + g2 * slab + o);
-                if (!pfirst) cpa(dst + VSZ + g2 * (VSZ / 2) + o, Q.vo + off0 + g2 * slab + o);
-              }
+            for (int o = lane * 2; o < VSZ / 2; o += 64) {
+              cpa(dst + g2 * (VSZ / 2) + o, Q.vi + off0 + g2 * slab + o);
+              if (p_vo) cpa(dst + VSZ + g2 * (VSZ / 2) + o, Q.vo + off0 + g2 * slab + o);
             }
-            const size_t ez = (size_t)(oct * Q.ngp + gp) * Q.nz;
-            if (wa == 0 && (fl & TF_X_IN)) {
-              const double* src = Q.fyz + ((ez + piz) * Q.ny + piy) * (size_t)ENT;
-              double* d2 = ringyz + (size_t)(wb * D + rs2) * ENT;
+          }
+          if (p_fyz) {
+            const double* src = p_fyz + (long long)p_dz * c2 * (long long)(Q.ny * ENT);
+            double* d2 = ringyz + (size_t)(wb * D + rs2) * ENT;
 #pragma unroll
-              for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
-            }
-            if (wb == 0 && (fl & TF_Y_IN)) {
-              const double* src = Q.fxz + ((ez + piz) * Q.nx + pix) * (size_t)ENT;
-              double* d2 = ringxz + (size_t)(wa * D + rs2) * ENT;
+            for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
+          }
+          if (p_fxz) {
+            const double* src = p_fxz + (long long)p_dz * c2 * (long long)(Q.nx * ENT);
+            double* d2 = ringxz + (size_t)(wa * D + rs2) * ENT;
 #pragma unroll
-              for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
-            }
-            if (c2 == 0 && (fl & TF_Z_IN)) {
-              const size_t ey = (size_t)(oct * Q.ngp + gp) * Q.ny;
-              const double* src = Q.fxy + ((ey + piy) * Q.nx + pix) * (size_t)ENT;
-              double* d2 = bufxy + (size_t)warp * ENT;
+            for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
+          }
+          if (c2 == 0 && p_fxy) {
+            double* d2 = bufxy + (size_t)warp * ENT;
 #pragma unroll
-              for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
-            }
+            for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, p_fxy + o);
           }
         }
         cp_async_commit();
       }
 
       // ---------------------------------------------- finish / stop / start
-      while (kc < nknown &&
-             G >= desc[kc % NSLOT].start + wa + wb + (desc[kc % NSLOT].rec[TK_Z1] - desc[kc % NSLOT].rec[TK_Z0])) {
-        // every write of task kc by this warp is issued: report it finished
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sdone[kc % NSLOT]);
-        ++kc;
-        have = false;
+      for (;;) {
+        if (have && G >= c_hi) {
+          // every write of task kc by this warp is issued: report it finished
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sdone[kc % NSLOT]);
+          ++kc;
+          have = false;
+        } else if (!have && kc < nknown) {
+          load_compute();
+        } else {
+          break;
+        }
       }
       if (stop_step >= 0 && G >= stop_step) break;
 
-      if (kc < nknown && G >= desc[kc % NSLOT].start + wa + wb) {
-        const int qs = kc % NSLOT;
-        if (!have) {
-          // task kc's constants and matrices into registers
-          mbar_test_wait(&sfull[qs], (uint32_t)((kc / NSLOT) & 1));  // acquire the loader's writes
-          const ChainDesc& dd = desc[qs];
-          c_oct = dd.rec[TK_OCT];
-          c_gp = dd.rec[TK_GP];
-          c_flags = dd.rec[TK_FLAGS];
-          c_start = dd.start;
-          c_nzr = dd.rec[TK_Z1] - dd.rec[TK_Z0];
-          const int w = dd.rec[TK_X1] - dd.rec[TK_X0], h = dd.rec[TK_Y1] - dd.rec[TK_Y0];
-          const int dx = (c_oct & 1) ? -1 : 1, dy = (c_oct & 2) ? -1 : 1;
-          c_dz = (c_oct & 4) ? -1 : 1;
-          c_act = wa < w && wb < h;
-          c_first = (c_flags & TF_FIRST) != 0 && !Q.vo_add;
-          ix = dx > 0 ? dd.rec[TK_X0] + wa : dd.rec[TK_X1] - 1 - wa;
-          iy = dy > 0 ? dd.rec[TK_Y0] + wb : dd.rec[TK_Y1] - 1 - wb;
-          c_iz0 = c_dz > 0 ? dd.rec[TK_Z0] : dd.rec[TK_Z1] - 1;
-          const int g_col = 2 * c_gp + (q4 >> 2);
-          c_gval = g_col < Q.ne;
-          g_vo = 2 * c_gp + (r >> 1);
-          c_gvo = g_vo < Q.ne;
-          so = (double)(1 + c_oct);
-          so_r = 1.0 / so;  // rounded, as the reference's 1/(1+octant)
-          face_k = c_gval ? (double)d_scale_energy(Q.ie_base + g_col) * (double)d_scale_unknown(q4 & 3) * so : 0.0;
-          sp_xy = ix + 3 * iy + 2;
-          col = (size_t)NM_ * NU * (ix + (size_t)Q.nx * iy);
-          ent_z = (size_t)(c_oct * Q.ngp + c_gp) * Q.nz;
-          ent_y = (size_t)(c_oct * Q.ngp + c_gp) * Q.ny;
-          x_in = wa == 0 && (c_flags & TF_X_IN);
-          y_in = wb == 0 && (c_flags & TF_Y_IN);
-          z_in = (c_flags & TF_Z_IN) != 0;
-          x_out = wa == w - 1 && (c_flags & TF_X_OUT);
-          y_out = wb == h - 1 && (c_flags & TF_Y_OUT);
-          z_out = (c_flags & TF_Z_OUT) != 0;
-          gx = dx > 0 ? -1 : Q.nx;
-          gy = dy > 0 ? -1 : Q.ny;
-          gz = c_dz > 0 ? -1 : Q.nz;
-          const double* mat = mats + qs * C::MAT;
-#pragma unroll
-          for (int k = 0; k < KS; ++k)
-#pragma unroll
-            for (int t = 0; t < 4; ++t) b1r[k][t] = mat[(k * 4 + t) * 32 + lane];
-#pragma unroll
-          for (int mt = 0; mt < MT; ++mt)
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-#pragma unroll
-              for (int i = 0; i < 2; ++i) a2r[mt][t][i] = mat[KS * 4 * 32 + ((mt * 4 + t) * 2 + i) * 32 + lane];
-          have = true;
-        }
-        const int c = (int)(G - c_start - wa - wb);
+      if (have && G >= c_lo) {
+        const int c = (int)(G - c_lo);
         cp_async_wait<LA>();  // this thread's copies of step G have landed
         __syncwarp();         // ... and every lane's
         if (c_act) {
@@ -608,7 +634,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
           si[CI_NKNOWN] = assigned;
           progress_made = true;
         }
-        if (progress_made || kc < nknown) {
+        if (progress_made || have || kc < nknown) {
           idle_since = global_ns();
         } else if (!si[CI_STOPSET] && global_ns() - idle_since > P.sy.timeout_ns) {
           // nothing was posted within the budget (the loader could not post
@@ -623,7 +649,7 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
       named_barrier_sync(1, NW * 32);
       nknown = si[CI_NKNOWN];
       if (stop_step < 0 && si[CI_STOPSET]) stop_step = *s_stop;
-      if (!(kc < nknown)) __nanosleep(32);  // idle: nothing to compute yet
+      if (!have && !(kc < nknown)) __nanosleep(32);  // idle: nothing to compute yet
     }
     cp_async_wait<0>();  // no copy into shared memory outlives the CTA
   }
