@@ -441,6 +441,21 @@ def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict |
     b = msb.Batch(descs, autotune=True)
     create_s = time.time() - t0
     info = b.info()
+    # the planner's list-scheduling simulation (one worker per SM): SM time
+    # busy when the problems share one launch, and when each runs alone
+    singles_ms, singles_busy = [], []
+    for q in probs:
+        with msb.Batch([q], plan_nsm=info["nsm"]) as b1:
+            i1 = b1.info()
+        singles_ms.append(i1["sim_makespan"])
+        singles_busy.append(i1["sim_busy"])
+    sm_, sb_ = np.array(singles_ms), np.array(singles_busy)
+    sim = {"busy_batched": info["sim_busy"], "busy_one_at_a_time_work_weighted": float((sm_ * sb_).sum() / sm_.sum()),
+           "busy_one_at_a_time_min": float(sb_.min()),
+           "predicted_speedup_vs_unbatched": float(sm_.sum() / info["sim_makespan"]),
+           "note": "host-side list-scheduling simulation of the planner (task durations from their wavefront "
+                   "steps): one problem alone already keeps the SMs this busy, so a shared launch can recover "
+                   "at most the difference"}
     s = torch.cuda.Stream(device=dev)
     sh = s.cuda_stream
 
@@ -542,6 +557,7 @@ def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict |
                         for c in info["classes"]],
             "scratch_gb": info["scratch_bytes"] / 1e9, "scratch_needed_all_gb": info["scratch_needed_all"] / 1e9,
             "scratch_waits": info["npred"], "create_s": create_s, "autotune_ms": info["tune_ms"],
+            "sm_utilisation_simulated": sim,
             "clocks": clk,
             "note": "one persistent launch sweeps every problem; the face scratch of all problems at once "
                     "does not fit beside the state, so problems reuse the scratch of completed ones (device-side "

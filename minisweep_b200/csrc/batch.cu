@@ -30,12 +30,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <new>
 #include <queue>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -454,9 +456,21 @@ int plan_batch(BatchImpl& B, const msb_problem* probs, int n, const std::map<std
     const bool t24 = it != tile24.end() && it->second;
     B.probs[i].tx = t24 ? 2 : 4;
     B.probs[i].ty = t24 ? 4 : 2;
-    int rc = plan_problem(B.probs[i], B.nsm);
-    if (rc) return rc;
   }
+  // the problems' schedules are independent: build them on the host's cores
+  std::vector<int> prc(n, MSB_OK);
+  {
+    const int nthr = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&]() {
+        for (int i = next++; i < n; i = next++) prc[i] = plan_problem(B.probs[i], B.nsm);
+      });
+    for (auto& th : pool) th.join();
+  }
+  for (int i = 0; i < n; ++i)
+    if (prc[i]) return plan_problem(B.probs[i], B.nsm);  // again on this thread: its error message
   make_classes(B, tile24);
   if ((int)B.classes.size() > kMaxBatchClasses) return set_error(MSB_ERR_ARG, "batch: too many classes");
   size_t need = 0;

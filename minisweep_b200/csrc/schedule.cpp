@@ -17,7 +17,6 @@
 #include <algorithm>
 #include <array>
 #include <cstdint>
-#include <unordered_map>
 
 #include "internal.h"
 
@@ -37,24 +36,6 @@ Range half(int n, int bit) {
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
-struct Key {
-  int phase, gpb, level, gp, oct, ity, itx;
-  bool operator<(const Key& o) const {
-    if (phase != o.phase) return phase < o.phase;
-    if (gpb != o.gpb) return gpb < o.gpb;
-    if (level != o.level) return level < o.level;
-    if (gp != o.gp) return gp < o.gp;
-    if (oct != o.oct) return oct < o.oct;
-    if (ity != o.ity) return ity < o.ity;
-    return itx < o.itx;
-  }
-};
-
-inline uint64_t pack(int phase, int oct, int gp, int itx, int ity) {
-  return ((uint64_t)phase << 60) | ((uint64_t)oct << 56) | ((uint64_t)gp << 36) |
-         ((uint64_t)itx << 18) | (uint64_t)ity;
-}
-
 }  // namespace
 
 int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block, Schedule& out) {
@@ -70,59 +51,72 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
   out.tx = tx;
   out.ty = ty;
 
-  struct Item {
-    Key key;
-    std::array<int, MSB_TASK_INTS> r;
-    uint64_t id;
+  // Tiles per region along x and y (the largest over the regions), and a
+  // dense index (phase, octant, group pair, tile x, tile y) -> task.
+  int ntxm = 0, ntym = 0;
+  for (int reg = 0; reg < NOCTANT; ++reg) {
+    ntxm = std::max(ntxm, ceil_div(half(nx, reg & 1).hi - half(nx, reg & 1).lo, tx));
+    ntym = std::max(ntym, ceil_div(half(ny, (reg >> 1) & 1).hi - half(ny, (reg >> 1) & 1).lo, ty));
+  }
+  const size_t ndense = (size_t)NOCTANT * NOCTANT * ngp * ntxm * ntym;
+  if (ndense >= (size_t)1 << 31) return set_error(MSB_ERR_ARG, "schedule: too many tasks");
+  std::vector<int> index(ndense, -1);
+  auto dense = [&](int p, int o, int gp, int itx, int ity) -> size_t {
+    return ((((size_t)p * NOCTANT + o) * ngp + gp) * ntxm + itx) * ntym + ity;
   };
-  std::vector<Item> items;
+  auto find = [&](int p, int o, int gp, int itx, int ity) -> int { return index[dense(p, o, gp, itx, ity)]; };
 
+  // Tasks in launch order: (phase, block of gp_block group pairs, level of
+  // the tile along the octant's sweep direction, group pair, octant, tile row,
+  // tile column) -- generated in that order directly.
+  std::vector<int>& rec = out.rec;
+  long long n = 0;
   for (int p = 0; p < NOCTANT; ++p)
-    for (int o = 0; o < NOCTANT; ++o) {
-      const int reg = o ^ p;
-      const Range rx = half(nx, reg & 1), ry = half(ny, (reg >> 1) & 1), rz = half(nz, (reg >> 2) & 1);
-      if (rx.empty() || ry.empty() || rz.empty()) continue;
-      const int dx = (o & 1) ? -1 : 1, dy = (o & 2) ? -1 : 1;
-      const int ntx = ceil_div(rx.hi - rx.lo, tx), nty = ceil_div(ry.hi - ry.lo, ty);
-      for (int gp = 0; gp < ngp; ++gp)
-        for (int ity = 0; ity < nty; ++ity)
-          for (int itx = 0; itx < ntx; ++itx) {
-            Item it;
-            it.r.fill(-1);
-            int* r = it.r.data();
-            r[TK_OCT] = o;
-            r[TK_PHASE] = p;
-            r[TK_GP] = gp;
-            r[TK_X0] = rx.lo + itx * tx;
-            r[TK_X1] = std::min(rx.hi, rx.lo + (itx + 1) * tx);
-            r[TK_Y0] = ry.lo + ity * ty;
-            r[TK_Y1] = std::min(ry.hi, ry.lo + (ity + 1) * ty);
-            r[TK_Z0] = rz.lo;
-            r[TK_Z1] = rz.hi;
-            const int ax = dx > 0 ? itx : ntx - 1 - itx;
-            const int ay = dy > 0 ? ity : nty - 1 - ity;
-            r[TK_LEVEL] = ax + ay;
-            it.key = Key{p, gp / gp_block, ax + ay, gp, o, ity, itx};
-            it.id = pack(p, o, gp, itx, ity);
-            items.push_back(it);
+    for (int gb = 0; gb * gp_block < ngp; ++gb) {
+      int maxlevel = 0;
+      for (int o = 0; o < NOCTANT; ++o) {
+        const int reg = o ^ p;
+        const int ntx = ceil_div(half(nx, reg & 1).hi - half(nx, reg & 1).lo, tx);
+        const int nty = ceil_div(half(ny, (reg >> 1) & 1).hi - half(ny, (reg >> 1) & 1).lo, ty);
+        maxlevel = std::max(maxlevel, ntx + nty - 1);
+      }
+      for (int level = 0; level < maxlevel; ++level)
+        for (int gp = gb * gp_block; gp < std::min(ngp, (gb + 1) * gp_block); ++gp)
+          for (int o = 0; o < NOCTANT; ++o) {
+            const int reg = o ^ p;
+            const Range rx = half(nx, reg & 1), ry = half(ny, (reg >> 1) & 1), rz = half(nz, (reg >> 2) & 1);
+            if (rx.empty() || ry.empty() || rz.empty()) continue;
+            const int dx = (o & 1) ? -1 : 1, dy = (o & 2) ? -1 : 1;
+            const int ntx = ceil_div(rx.hi - rx.lo, tx), nty = ceil_div(ry.hi - ry.lo, ty);
+            for (int ity = 0; ity < nty; ++ity) {
+              const int ay = dy > 0 ? ity : nty - 1 - ity;
+              const int ax = level - ay;
+              if (ax < 0 || ax >= ntx) continue;
+              const int itx = dx > 0 ? ax : ntx - 1 - ax;
+              rec.resize(rec.size() + MSB_TASK_INTS, -1);
+              int* r = &rec[(size_t)n * MSB_TASK_INTS];
+              r[TK_OCT] = o;
+              r[TK_PHASE] = p;
+              r[TK_GP] = gp;
+              r[TK_X0] = rx.lo + itx * tx;
+              r[TK_X1] = std::min(rx.hi, rx.lo + (itx + 1) * tx);
+              r[TK_Y0] = ry.lo + ity * ty;
+              r[TK_Y1] = std::min(ry.hi, ry.lo + (ity + 1) * ty);
+              r[TK_Z0] = rz.lo;
+              r[TK_Z1] = rz.hi;
+              r[TK_LEVEL] = level;
+              index[dense(p, o, gp, itx, ity)] = (int)n;
+              ++n;
+            }
           }
     }
 
-  std::sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.key < b.key; });
-  std::unordered_map<uint64_t, int> index;
-  index.reserve(items.size() * 2);
-  for (size_t i = 0; i < items.size(); ++i) index[items[i].id] = (int)i;
-  auto find = [&](int p, int o, int gp, int itx, int ity) -> int {
-    auto f = index.find(pack(p, o, gp, itx, ity));
-    return f == index.end() ? -1 : f->second;
-  };
-
-  out.rec.resize(items.size() * MSB_TASK_INTS);
-  for (size_t i = 0; i < items.size(); ++i) {
-    int* r = items[i].r.data();
+  // Dependencies; every one points to an earlier task.
+  for (long long i = 0; i < n; ++i) {
+    int* r = &rec[(size_t)i * MSB_TASK_INTS];
     const int o = r[TK_OCT], p = r[TK_PHASE], gp = r[TK_GP];
     const int reg = o ^ p;
-    const int dx = (o & 1) ? -1 : 1, dy = (o & 2) ? -1 : 1, dz = (o & 4) ? -1 : 1;
+    const int dx = (o & 1) ? -1 : 1, dy = (o & 2) ? -1 : 1;
     const Range rx = half(nx, reg & 1), ry = half(ny, (reg >> 1) & 1);
     const int ntx = ceil_div(rx.hi - rx.lo, tx), nty = ceil_div(ry.hi - ry.lo, ty);
     const int itx = (r[TK_X0] - rx.lo) / tx, ity = (r[TK_Y0] - ry.lo) / ty;
@@ -135,15 +129,11 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
       if (!first_in_reg) {
         r[TK_DEP_X] = find(p, o, gp, itx - dx, ity);
         mode |= DM_X_PLANE;
-      } else {
+      } else if ((p >> 0) & 1) {
         // the other x-half is upwind iff this region is on the downwind half
-        const bool downwind_half = ((p >> 0) & 1) != 0;
-        if (downwind_half) {
-          const int preg = reg ^ 1;
-          const Range px = half(nx, preg & 1);
-          const int pntx = ceil_div(px.hi - px.lo, tx);
-          r[TK_DEP_X] = find(p ^ 1, o, gp, dx > 0 ? pntx - 1 : 0, ity);
-        }
+        const Range px = half(nx, (reg ^ 1) & 1);
+        const int pntx = ceil_div(px.hi - px.lo, tx);
+        if (!px.empty()) r[TK_DEP_X] = find(p ^ 1, o, gp, dx > 0 ? pntx - 1 : 0, ity);
       }
       if (r[TK_DEP_X] >= 0) flags |= TF_X_IN;
       const bool has_down = !last_in_reg || (((p >> 0) & 1) == 0 && !half(nx, (reg ^ 1) & 1).empty());
@@ -156,14 +146,10 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
       if (!first_in_reg) {
         r[TK_DEP_Y] = find(p, o, gp, itx, ity - dy);
         mode |= DM_Y_PLANE;
-      } else {
-        const bool downwind_half = ((p >> 1) & 1) != 0;
-        if (downwind_half) {
-          const int preg = reg ^ 2;
-          const Range py = half(ny, (preg >> 1) & 1);
-          const int pnty = ceil_div(py.hi - py.lo, ty);
-          r[TK_DEP_Y] = find(p ^ 2, o, gp, itx, dy > 0 ? pnty - 1 : 0);
-        }
+      } else if ((p >> 1) & 1) {
+        const Range py = half(ny, ((reg ^ 2) >> 1) & 1);
+        const int pnty = ceil_div(py.hi - py.lo, ty);
+        if (!py.empty()) r[TK_DEP_Y] = find(p ^ 2, o, gp, itx, dy > 0 ? pnty - 1 : 0);
       }
       if (r[TK_DEP_Y] >= 0) flags |= TF_Y_IN;
       const bool has_down = !last_in_reg || (((p >> 1) & 1) == 0 && !half(ny, ((reg ^ 2) >> 1) & 1).empty());
@@ -176,7 +162,6 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
       if (downwind_half) r[TK_DEP_Z] = find(p ^ 4, o, gp, itx, ity);
       if (r[TK_DEP_Z] >= 0) flags |= TF_Z_IN;
       if (!downwind_half && !half(nz, ((reg ^ 4) >> 2) & 1).empty()) flags |= TF_Z_OUT;
-      (void)dz;
     }
     // ---- vo order: previous visitor of this tile (phase p-1, octant reg^(p-1))
     if (p == 0) {
@@ -189,7 +174,6 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
     r[TK_DEP_MODE] = mode;
     for (int d = TK_DEP_X; d <= TK_DEP_VO; ++d)
       if (r[d] >= (int)i) return set_error(MSB_ERR_ARG, "schedule: dependency not topological");
-    std::copy(r, r + MSB_TASK_INTS, out.rec.begin() + i * MSB_TASK_INTS);
   }
   return MSB_OK;
 }
