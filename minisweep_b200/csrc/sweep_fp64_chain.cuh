@@ -16,10 +16,9 @@
 // always of the same task and plane, whichever tasks the warps are in.
 //
 // Per step a compute warp
-//   * issues copies of what it needs LA steps later: vi and the previous vo
-//     of its cell with 16-byte cp.async, the face entering the tile at its x-
-//     or y-upwind edge and the face entering at the task's first plane with
-//     one 1-D bulk copy each (completed on a per-buffer mbarrier);
+//   * issues 16-byte cp.async copies of what it needs LA steps later: vi and
+//     the previous vo of its cell, the face entering the tile at its x- or
+//     y-upwind edge, the face entering at the task's first plane;
 //   * waits for its own copies of this step, solves its cell (FP64
 //     tensor-core transforms mma.sync m8n8k4 f64, Quantities_solve on
 //     registers, z face carried in registers), writes its x / y faces into
@@ -95,9 +94,7 @@ struct ChainCfg {
   static constexpr int SM_DESC = SM_MAT + NSLOT * MAT;      // [NSLOT] ChainDesc
   static constexpr int DESC_D = (int)(sizeof(ChainDesc) / sizeof(double));
   static constexpr int SM_BAR = SM_DESC + NSLOT * DESC_D;   // full[NSLOT], done[NSLOT], free[NSLOT]
-  static constexpr int NFBAR = TY * D + TX * D + NW;        // face copies: yz ring, xz ring, xy buffer
-  static constexpr int SM_FBAR = SM_BAR + 3 * NSLOT;        // [NFBAR] mbarriers of the face copies
-  static constexpr int SM_INT = SM_FBAR + NFBAR;            // shared ints and the stop step (4 doubles)
+  static constexpr int SM_INT = SM_BAR + 3 * NSLOT;         // shared ints and the stop step (4 doubles)
   static constexpr int SM_END = SM_INT + 4;
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)SM_END; }
   static_assert(sizeof(ChainDesc) % sizeof(double) == 0, "desc size");
@@ -135,10 +132,6 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
   uint64_t* const sfull = reinterpret_cast<uint64_t*>(smem + C::SM_BAR);
   uint64_t* const sdone = sfull + NSLOT;
   uint64_t* const sfree = sdone + NSLOT;
-  // one mbarrier per face buffer: the bulk copy into it completes the phase
-  uint64_t* const fbar_yz = reinterpret_cast<uint64_t*>(smem + C::SM_FBAR);  // [TY][D]
-  uint64_t* const fbar_xz = fbar_yz + TY * D;                                 // [TX][D]
-  uint64_t* const fbar_xy = fbar_xz + TX * D;                                 // [NW]
   volatile int* const si = reinterpret_cast<volatile int*>(smem + C::SM_INT);
   volatile long long* const s_stop = reinterpret_cast<volatile long long*>(smem + C::SM_INT + kChainStopSlot);
 
@@ -153,7 +146,6 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
       mbar_init(&sdone[i], NW);  // every compute warp, after its last plane of the task
       mbar_init(&sfree[i], 1);   // the publisher, after publishing the task
     }
-    for (int i = 0; i < C::NFBAR; ++i) mbar_init(&fbar_yz[i], 1);  // the issuing lane's expect_tx
     si[CI_NKNOWN] = 0;
     si[CI_FINAL] = -1;
     si[CI_STOPSET] = 0;
@@ -339,10 +331,6 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
       p_fyz = (wa == 0 && (fl & TF_X_IN)) ? Q.fyz + ((eo * Q.nz + piz0) * Q.ny + piy) * (size_t)ENT : nullptr;
       p_fxz = (wb == 0 && (fl & TF_Y_IN)) ? Q.fxz + ((eo * Q.nz + piz0) * Q.nx + pix) * (size_t)ENT : nullptr;
       p_fxy = (fl & TF_Z_IN) ? Q.fxy + ((eo * Q.ny + piy) * Q.nx + pix) * (size_t)ENT : nullptr;
-      // the task's entering faces were written by generic stores of other
-      // CTAs (published before the task was posted); the bulk copies read
-      // them through the async proxy
-      fence_proxy_async();
       p_have = true;
     };
 
@@ -412,9 +400,6 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
       have = true;
     };
 
-    // phase parity of this warp's face-copy mbarriers: bit slot (yz ring),
-    // D + slot (xz ring), 2 D (xy buffer)
-    uint32_t fph = 0;
     long long G = 0;
     int rs = 0;  // G % D
     for (;; ++G, rs = rs + 1 == D ? 0 : rs + 1) {
@@ -447,28 +432,22 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
               if (p_vo) cpa(dst + VSZ + g2 * (VSZ / 2) + o, Q.vo + off0 + g2 * slab + o);
             }
           }
-          // the faces entering at this warp's tile edges: one 1-D bulk copy
-          // each, completed on the buffer's mbarrier
-          if (lane == 0 && (p_fyz || p_fxz || (c2 == 0 && p_fxy))) {
-            // the buffer was last read by generic loads of this warp
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            if (p_fyz) {
-              uint64_t* b = &fbar_yz[wb * D + rs2];
-              mbar_arrive_expect_tx(b, ENT * 8);
-              bulk_g2s(ringyz + (size_t)(wb * D + rs2) * ENT,
-                       p_fyz + (long long)p_dz * c2 * (long long)(Q.ny * ENT), ENT * 8, b);
-            }
-            if (p_fxz) {
-              uint64_t* b = &fbar_xz[wa * D + rs2];
-              mbar_arrive_expect_tx(b, ENT * 8);
-              bulk_g2s(ringxz + (size_t)(wa * D + rs2) * ENT,
-                       p_fxz + (long long)p_dz * c2 * (long long)(Q.nx * ENT), ENT * 8, b);
-            }
-            if (c2 == 0 && p_fxy) {
-              uint64_t* b = &fbar_xy[warp];
-              mbar_arrive_expect_tx(b, ENT * 8);
-              bulk_g2s(bufxy + (size_t)warp * ENT, p_fxy, ENT * 8, b);
-            }
+          if (p_fyz) {
+            const double* src = p_fyz + (long long)p_dz * c2 * (long long)(Q.ny * ENT);
+            double* d2 = ringyz + (size_t)(wb * D + rs2) * ENT;
+#pragma unroll
+            for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
+          }
+          if (p_fxz) {
+            const double* src = p_fxz + (long long)p_dz * c2 * (long long)(Q.nx * ENT);
+            double* d2 = ringxz + (size_t)(wa * D + rs2) * ENT;
+#pragma unroll
+            for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, src + o);
+          }
+          if (c2 == 0 && p_fxy) {
+            double* d2 = bufxy + (size_t)warp * ENT;
+#pragma unroll
+            for (int o = lane * 2; o < ENT; o += 64) cpa(d2 + o, p_fxy + o);
           }
         }
         cp_async_commit();
@@ -495,20 +474,6 @@ __global__ void __launch_bounds__((TX * TY + 4) * 32, 1) sweep_fp64_chain_kernel
         cp_async_wait<LA>();  // this thread's copies of step G have landed
         __syncwarp();         // ... and every lane's
         if (c_act) {
-          // the faces entering at this warp's tile edges have landed (a wait
-          // that runs out records the error; the sweep then ends)
-          if (x_in) {
-            mbar_wait(&fbar_yz[wb * D + rs], (fph >> rs) & 1u, P.sy, -1);
-            fph ^= 1u << rs;
-          }
-          if (y_in) {
-            mbar_wait(&fbar_xz[wa * D + rs], (fph >> (D + rs)) & 1u, P.sy, -1);
-            fph ^= 1u << (D + rs);
-          }
-          if (c == 0 && z_in) {
-            mbar_wait(&fbar_xy[warp], (fph >> (2 * D)) & 1u, P.sy, -1);
-            fph ^= 1u << (2 * D);
-          }
           const int iz = c_iz0 + c_dz * c;
           const int dx = (c_oct & 1) ? -1 : 1, dy = (c_oct & 2) ? -1 : 1, dz = c_dz;
           const double* const vst = ringv + (size_t)(warp * D + rs) * 2 * VSZ;
