@@ -570,14 +570,15 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     import minisweep_b200 as msb
     from minisweep_b200.parallel import max_over_ranks, sum_norms
 
+    # this rank's GPU first: the NCCL communicator binds to the current device
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
     dist = None
     if world > 1:
         import datetime
 
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
 
     def barrier():
         torch.cuda.synchronize()
