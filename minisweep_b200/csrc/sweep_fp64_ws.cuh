@@ -124,8 +124,11 @@ struct Fp64Cfg {
   // With 8 compute warps the launch gives every thread 65536 / 384 = 168
   // registers; the producer warpgroup hands most of its share to them.
   static constexpr bool REBALANCE = NW == 8;
-  static constexpr int REG_PRODUCER = 96;
-  static constexpr int REG_COMPUTE = 200;  // 8*32*200 + 4*32*96 <= 384 * 168
+  // measured at 64^3 x ne 64: 208 / 80 gives 118.0 ms per sweep, 200 / 96
+  // 121.1 ms (the compute warps spill below ~200)
+  static constexpr int REG_PRODUCER = 80;
+  static constexpr int REG_COMPUTE = 208;  // 8*32*208 + 4*32*80 <= 384 * 168; per SMSP 2*208 + 80 <= 512
+  static_assert(!REBALANCE || NW * 32 * REG_COMPUTE + 4 * 32 * REG_PRODUCER <= NT * 168, "register split");
   static constexpr int ENT = NCH * 256;     // doubles per face entry
   static constexpr bool FACE_PF = NCH == 1; // faces entering the tile staged by the producer
   static constexpr int NXY = TY;  // first-plane xy faces staged per step: one per row
@@ -813,12 +816,17 @@ __device__ __forceinline__ void fp64_batch_switch(const Fp64Batch& P, int c) {
 // them so), and the kernel visits the kinds in that order, one straight-line
 // region per kind: compiled as separate regions (rather than the cases of a
 // switch) the bodies keep their register allocations apart.
+// Register split of the batched kernel (all class bodies in one kernel):
+// 200 / 96 (its producer code spills with the single-problem kernel's 80).
+constexpr int kBatchRegCompute = 200, kBatchRegProducer = 96;
+static_assert(8 * 32 * kBatchRegCompute + 4 * 32 * kBatchRegProducer <= 12 * 32 * 168, "batch register split");
+
 template <int NS>
 __global__ void __launch_bounds__(12 * 32, 1) sweep_fp64_batch_kernel(const Fp64Batch P) {
   if (blockIdx.x == 0 && threadIdx.x == 0) P.ptime[P.nprob] = global_ns();
   // the register split of the 8-compute-warp bodies, once for all classes
   if ((threadIdx.x >> 5) >= 8) {
-    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Fp64Cfg<16, 1, 4, 2, NS>::REG_PRODUCER));
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kBatchRegProducer));
     int c = 0;
 #define MSB_K(K, NM, NCH, TX, TY)                                 \
   if (c < P.nclass && P.cls_kind[c] == K) {                       \
@@ -829,7 +837,7 @@ __global__ void __launch_bounds__(12 * 32, 1) sweep_fp64_batch_kernel(const Fp64
     MSB_FP64_BATCH_KINDS(MSB_K)
 #undef MSB_K
   } else {
-    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Fp64Cfg<16, 1, 4, 2, NS>::REG_COMPUTE));
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kBatchRegCompute));
     int c = 0;
 #define MSB_K(K, NM, NCH, TX, TY)                                 \
   if (c < P.nclass && P.cls_kind[c] == K) {                       \
