@@ -163,10 +163,11 @@ __device__ __forceinline__ void fp64_barriers(bool init) {
   if (init) {
     for (int i = 0; i < NS; ++i) {
       mbar_init(&bars[i], 1);            // full: the loader's arrive.expect_tx (header + face copies)
-      mbar_init(&bars[NS + i], C::NW);   // done: every compute warp
+      mbar_init(&bars[NS + i], 1);       // done: compute warp 0, after the compute warps' step barrier
       mbar_init(&bars[2 * NS + i], 1);   // freed: the publisher
     }
     *reinterpret_cast<volatile int*>(smem + C::SM_FINAL) = -1;
+    reinterpret_cast<volatile int*>(smem + C::SM_FINAL)[1] = 0;  // compute warps' quit flag
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   } else {
     for (int i = 0; i < 3 * NS; ++i) mbar_inval(&bars[i]);
@@ -500,12 +501,23 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
   double carry[NCH][4][2];
   double d1n[NCH][4][2];  // angle values of the next plane (PIPE_T1)
 
+  // The compute warps meet at a hardware barrier (bar.sync 1) once per step
+  // and once per task start.  Every exit is decided uniformly: a warp whose
+  // bounded wait ran out, or that finds the stop header, raises s_quit before
+  // the barrier, and all warps leave after it; no warp leaves the others at a
+  // barrier.
+  volatile int& s_quit = reinterpret_cast<volatile int*>(smem + C::SM_FINAL)[1];
   long long G = 0;
   for (;;) {
     // ------------------------------------------------ one task per iteration
-    if (!mbar_wait(&full[G % NS], (uint32_t)((G / NS) & 1), P.sy, -1)) break;
+    {
+      const bool ok = mbar_wait(&full[G % NS], (uint32_t)((G / NS) & 1), P.sy, -1);
+      const StepHdr* h0 = reinterpret_cast<const StepHdr*>(stages + (size_t)(G % NS) * C::STAGE + C::ST_HDR);
+      if (lane == 0 && (!ok || h0->stop)) s_quit = 1;
+      asm volatile("bar.sync 1, %0;" ::"n"(NW * 32) : "memory");
+      if (s_quit) break;
+    }
     const StepHdr* hdr0 = reinterpret_cast<const StepHdr*>(stages + (size_t)(G % NS) * C::STAGE + C::ST_HDR);
-    if (hdr0->stop) break;
     const int oct = hdr0->oct, gp = hdr0->gp, flags = hdr0->flags;
     const int x0 = hdr0->x0, x1 = hdr0->x1, y0 = hdr0->y0, y1 = hdr0->y1, z0 = hdr0->z0, z1 = hdr0->z1;
     const double* mat = mats + hdr0->mat * C::MAT;
@@ -600,10 +612,13 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
     for (int s = 0; s < nsteps; ++s, ++G) {
       const int st = (int)(G % NS);
       const double* stg = stages + (size_t)st * C::STAGE;
+      bool go = true;  // this warp computes step G
       if (s > 0) {
-        if (!mbar_wait(&full[st], (uint32_t)((G / NS) & 1), P.sy, -1)) { stop = true; break; }
-        if (reinterpret_cast<const StepHdr*>(stg + C::ST_HDR)->stop) { stop = true; break; }
+        go = mbar_wait(&full[st], (uint32_t)((G / NS) & 1), P.sy, -1) &&
+             !reinterpret_cast<const StepHdr*>(stg + C::ST_HDR)->stop;
+        if (!go && lane == 0) s_quit = 1;
       }
+      if (go) {
       prefetch(s + 3, G + 3);
       cp_async_wait<2>();  // the groups of steps s and s+1 have landed (this thread's copies)
       __syncwarp();        // ... and every lane's
@@ -751,12 +766,14 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
             }
         }
       }
-      // step G done by this warp: its writes are ordered before the arrive;
-      // once every compute warp has arrived, the neighbours' faces of step G
-      // are visible and step G + 1 may start
+      }  // go
+      // step G done by every compute warp: their writes are ordered before
+      // the barrier, the neighbours' faces of step G are visible and step
+      // G + 1 may start; warp 0 then tells the publisher
       __syncwarp();
-      if (lane == 0) mbar_arrive(&done[st]);
-      if (!mbar_wait(&done[st], (uint32_t)((G / NS) & 1), P.sy, -1)) { stop = true; break; }
+      asm volatile("bar.sync 1, %0;" ::"n"(NW * 32) : "memory");
+      if (s_quit) { stop = true; break; }
+      if (warp == 0 && lane == 0) mbar_arrive(&done[st]);
     }
     if (stop) break;
   }
