@@ -130,11 +130,15 @@ Bool_t Arguments_are_all_consumed(const Arguments* args);
 
 /*======================================================================= env
  * src/1_base/env_types.h:54-70, env.h:46-80, env_mpi.h, env_cuda.h.
- * One process drives one GPU: the process grid is 1 x 1. */
+ * One process drives one GPU.  The process grid is 1 x 1 unless the host
+ * program gave the Env a process group (msb_env_set_comm, below), the
+ * counterpart of the reference's MPI_COMM_WORLD (env_mpi.c:100-141). */
 typedef int Comm_t;
 typedef int Request_t;
 typedef void* Stream_t; /* a cudaStream_t */
 typedef double Timer;
+
+typedef struct msb_comm msb_comm;
 
 typedef struct {
   int nproc_x_;
@@ -144,7 +148,10 @@ typedef struct {
   Bool_t is_using_device_;
   Stream_t stream_kernel_faces_;
   int device_;
-  int pad;
+  int proc_;         /* this process's number in its group (0 without one) */
+  int nproc_world_;  /* processes in the group (1 without one)             */
+  int pad_;
+  const msb_comm* comm_;
 } Env;
 
 Env Env_null(void);
@@ -464,6 +471,80 @@ int msb_batch_set_spin_limit(msb_batch* b, long long limit);
 /* The built-in transform matrices (Quantities_init_am_matrices_,
  * quantities_testing_c.h:40-201) for nm moments and na angles, 8 octants. */
 int msb_builtin_matrices(int nm, int na, double* a_from_m, double* m_from_a);
+
+/*------------------------------------------------------- KBA decomposition
+ * --nproc_x / --nproc_y > 1: the x-y plane is split over a process grid, one
+ * process (one GPU) per subdomain, as the reference's MPI build does
+ * (runner.c:95-106 sizes, quantities_testing_c.h:206-333 offsets,
+ * stepscheduler_kba.c:80-284 steps, faces_kba.c:86-479 face exchange).  A
+ * sweep is a sequence of steps; at each step every process sweeps one
+ * (octant, z-block) slab of its subdomain with one kernel launch, then the
+ * faces leaving the slab cross to the downwind neighbours.  The transport is
+ * the host program's: it hands the Env a table of callbacks (MPI, NCCL
+ * through torch.distributed, ...), the counterpart of the reference's
+ * Env_send / Env_recv / Env_sum_d over MPI_COMM_WORLD (env_mpi.c:309-480). */
+typedef struct {
+  int peer;      /* process number of the other side                         */
+  int is_send;   /* 1: send `bytes` of buf to peer; 0: receive them into buf */
+  int axis;      /* 0: x faces (yz planes), 1: y faces (xz planes)           */
+  int side;      /* the peer's position along the axis: 0 lower, 1 higher    */
+  size_t bytes;
+  void* buf;     /* device memory of this process                            */
+} msb_kba_msg;
+
+struct msb_comm {
+  void* ctx;
+  /* Every process calls this after each step with the messages of that step
+   * (possibly none) and returns 0 once its receives have landed in device
+   * memory.  The device work that filled the send buffers has finished. */
+  int (*exchange)(void* ctx, const msb_kba_msg* msgs, int nmsg);
+  /* The collectives run over the active processes 0 .. nactive - 1 (the
+   * reference's active communicator, env_mpi.c:128-135), called by each of
+   * them.  sum_double: *value = the sum of their *value (Env_sum_d).
+   * allgather_int: values[p] = the value of process p.  A transport that
+   * serves only the whole group returns nonzero for nactive < nproc. */
+  int (*sum_double)(void* ctx, int nactive, double* value);
+  int (*allgather_int)(void* ctx, int nactive, int value, int* values);
+  int (*barrier)(void* ctx, int nactive);
+};
+
+/* Before Env_set_values: this process is number `proc` of `nproc`, reached
+ * through `comm` (which must outlive the Env).  Env_set_values then accepts
+ * any grid of up to nproc processes; processes numbered beyond it are
+ * inactive (env_mpi.c:119-135). */
+int msb_env_set_comm(Env* env, int proc, int nproc, const msb_comm* comm);
+
+/* Host-only: the step plan of a decomposed sweep.  Unit k (0 <= k <
+ * 8 * nblock_z) is octant unit_oct[k] on z-block unit_zb[k]; process p sweeps
+ * it at step start[p * 8 * nblock_z + k]; nstep steps in all.  Arrays may be
+ * NULL. */
+int msb_kba_plan(int nproc_x, int nproc_y, int nblock_z, int* nstep, int* unit_oct, int* unit_zb, int* start);
+/* Host-only: the messages of process `proc` after step `step`, 5 ints each
+ * (peer, is_send, axis, side, unit); returns their count. */
+int msb_kba_plan_messages(int nproc_x, int nproc_y, int nblock_z, int proc, int step, int* out, int max_msgs);
+
+/* A decomposed sweep driven step by step, for hosts that run the exchange
+ * themselves (Sweeper_sweep does all of it through the Env's callbacks).
+ * Sweeper created with an Env whose grid is nproc_x x nproc_y > 1.
+ *   msb_kba_info: steps per sweep; bytes of the largest message per axis.
+ *   msb_kba_set_buffers: device buffers for the messages (send x, send y,
+ *     then receives x from the lower / higher neighbour, y lower / higher),
+ *     each at least the axis's bytes; NULL = buffers the sweeper allocates.
+ *   msb_kba_begin: starts vo_d = sweep(vi_d) on the Env's stream.
+ *   msb_kba_step: launches this process's slab of `step` (if any) and copies
+ *     its leaving faces into the send buffers.
+ *   msb_kba_messages: the step's messages with their buffers.
+ *   msb_kba_unpack: after the receives of `step` landed: the entering faces
+ *     into this process's face planes.
+ *   msb_kba_end: waits for the device work; the sweep's status. */
+int msb_kba_info(const Sweeper* sweeper, int* nstep, size_t* bytes_x, size_t* bytes_y);
+int msb_kba_set_buffers(Sweeper* sweeper, void* send_x, void* send_y, void* recv_x_lo, void* recv_x_hi,
+                        void* recv_y_lo, void* recv_y_hi);
+int msb_kba_begin(Sweeper* sweeper, double* vo_d, const double* vi_d, const Quantities* quan, Env* env);
+int msb_kba_step(Sweeper* sweeper, int step, Env* env);
+int msb_kba_messages(const Sweeper* sweeper, int step, msb_kba_msg* msgs, int max_msgs);
+int msb_kba_unpack(Sweeper* sweeper, int step, Env* env);
+int msb_kba_end(Sweeper* sweeper, Env* env);
 
 #ifdef __cplusplus
 }

@@ -42,7 +42,27 @@ class Arguments(ctypes.Structure):
 class Env(ctypes.Structure):
     _fields_ = [("nproc_x_", ctypes.c_int), ("nproc_y_", ctypes.c_int), ("tag_", ctypes.c_int),
                 ("is_proc_active_", ctypes.c_int), ("is_using_device_", ctypes.c_int),
-                ("stream_kernel_faces_", ctypes.c_void_p), ("device_", ctypes.c_int), ("pad", ctypes.c_int)]
+                ("stream_kernel_faces_", ctypes.c_void_p), ("device_", ctypes.c_int), ("proc_", ctypes.c_int),
+                ("nproc_world_", ctypes.c_int), ("pad_", ctypes.c_int), ("comm_", ctypes.c_void_p)]
+
+
+class KbaMsg(ctypes.Structure):
+    """msb_kba_msg: one face slab crossing between neighbouring processes."""
+    _fields_ = [("peer", ctypes.c_int), ("is_send", ctypes.c_int), ("axis", ctypes.c_int), ("side", ctypes.c_int),
+                ("bytes", ctypes.c_size_t), ("buf", ctypes.c_void_p)]
+
+
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(KbaMsg), ctypes.c_int)
+SUM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
+ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_int))
+BARRIER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int)
+
+
+class Comm(ctypes.Structure):
+    """msb_comm: the process group's transport, as C callbacks."""
+    _fields_ = [("ctx", ctypes.c_void_p), ("exchange", EXCHANGE_FN), ("sum_double", SUM_FN),
+                ("allgather_int", ALLGATHER_FN), ("barrier", BARRIER_FN)]
 
 
 class Pointer(ctypes.Structure):
@@ -142,6 +162,17 @@ def lib() -> ctypes.CDLL:
                                         P(ctypes.c_int), P(ctypes.c_int), ctypes.c_int]
         L.msb_batch_set_spin_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
         L.msb_builtin_matrices.argtypes = [ctypes.c_int, ctypes.c_int, P(D), P(D)]
+        L.msb_env_set_comm.argtypes = [P(Env), ctypes.c_int, ctypes.c_int, P(Comm)]
+        IP = P(ctypes.c_int)
+        L.msb_kba_plan.argtypes = [ctypes.c_int] * 3 + [IP] * 4
+        L.msb_kba_plan_messages.argtypes = [ctypes.c_int] * 5 + [IP, ctypes.c_int]
+        L.msb_kba_info.argtypes = [P(Sweeper), IP, P(ctypes.c_size_t), P(ctypes.c_size_t)]
+        L.msb_kba_set_buffers.argtypes = [P(Sweeper)] + [ctypes.c_void_p] * 6
+        L.msb_kba_begin.argtypes = [P(Sweeper), ctypes.c_void_p, ctypes.c_void_p, P(Quantities), P(Env)]
+        L.msb_kba_step.argtypes = [P(Sweeper), ctypes.c_int, P(Env)]
+        L.msb_kba_messages.argtypes = [P(Sweeper), ctypes.c_int, P(KbaMsg), ctypes.c_int]
+        L.msb_kba_unpack.argtypes = [P(Sweeper), ctypes.c_int, P(Env)]
+        L.msb_kba_end.argtypes = [P(Sweeper), P(Env)]
         L.initialize_state.argtypes = [P(D), Dimensions, ctypes.c_int, P(Quantities)]
         L.get_state_norms.argtypes = [P(D), P(D), Dimensions, ctypes.c_int, P(D), P(D), P(Env)]
         _lib = L
@@ -174,6 +205,80 @@ def schedule(nx, ny, nz, ne, tx=4, ty=2, gp_block=1) -> np.ndarray:
     return out
 
 
+def kba_plan(nproc_x: int, nproc_y: int, nblock_z: int):
+    """Step plan of a decomposed sweep (host only): (nstep, unit_oct, unit_zb,
+    start[proc, unit]).  Unit k is octant unit_oct[k] on z-block unit_zb[k]."""
+    L = lib()
+    IP = ctypes.POINTER(ctypes.c_int)
+    nunit = NOCTANT * nblock_z
+    nstep = ctypes.c_int()
+    oct_ = np.zeros(nunit, dtype=np.int32)
+    zb = np.zeros(nunit, dtype=np.int32)
+    start = np.zeros((nproc_x * nproc_y, nunit), dtype=np.int32)
+    _check(L.msb_kba_plan(nproc_x, nproc_y, nblock_z, ctypes.byref(nstep), oct_.ctypes.data_as(IP),
+                          zb.ctypes.data_as(IP), start.ctypes.data_as(IP)))
+    return nstep.value, oct_, zb, start
+
+
+def kba_plan_messages(nproc_x: int, nproc_y: int, nblock_z: int, proc: int, step: int):
+    """Messages of process `proc` after step `step` (host only): a list of
+    dicts peer / is_send / axis / side / unit."""
+    out = np.zeros(5 * 8, dtype=np.int32)
+    n = lib().msb_kba_plan_messages(nproc_x, nproc_y, nblock_z, proc, step,
+                                    out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 8)
+    if n < 0:
+        raise SweepError(n, last_error())
+    keys = ("peer", "is_send", "axis", "side", "unit")
+    return [dict(zip(keys, (int(v) for v in out[5 * i:5 * i + 5]))) for i in range(n)]
+
+
+def local_extent(n_global: int, nproc: int, proc: int):
+    """(offset, size) of process `proc`'s share of n_global cells along one
+    axis, as the reference's driver splits it (runner.c:95-106)."""
+    lo, hi = (proc * n_global) // nproc, ((proc + 1) * n_global) // nproc
+    return lo, hi - lo
+
+
+def make_comm(exchange, sum_double, allgather_int, barrier) -> Comm:
+    """msb_comm from Python callables: exchange(msgs) with msgs a list of
+    KbaMsg; sum_double(nactive, x) -> float; allgather_int(nactive, v) ->
+    list of ints; barrier(nactive) -- the collectives over the active
+    processes 0 .. nactive - 1.  A callable that raises makes the call return
+    -1.  Keep the result alive as long as an Env uses it (it holds the
+    callbacks)."""
+    import traceback
+
+    def guard(fn):
+        def call(*a):
+            try:
+                return fn(*a)
+            except Exception:  # the C caller only sees the status
+                traceback.print_exc()
+                return -1
+        return call
+
+    def ex(_ctx, msgs, n):
+        exchange([msgs[i] for i in range(n)])
+        return 0
+
+    def sm(_ctx, nactive, v):
+        v[0] = float(sum_double(nactive, v[0]))
+        return 0
+
+    def ag(_ctx, nactive, value, out):
+        vals = allgather_int(nactive, int(value))
+        for i, x in enumerate(vals):
+            out[i] = int(x)
+        return 0
+
+    def br(_ctx, nactive):
+        barrier(nactive)
+        return 0
+
+    c = Comm(None, EXCHANGE_FN(guard(ex)), SUM_FN(guard(sm)), ALLGATHER_FN(guard(ag)), BARRIER_FN(guard(br)))
+    return c
+
+
 def fp64_peak(reps: int = 5):
     """Measured FP64 throughput of this GPU (TFLOP/s): (tensor-core mma, FMA pipe)."""
     a, b = ctypes.c_double(), ctypes.c_double()
@@ -200,16 +305,28 @@ class Problem:
     """One sweep problem driven through the reference-compatible C API:
     Env + Quantities (built-in) + Sweeper created from a reference flag string."""
 
-    def __init__(self, argstring: str, nm: int = 16):
+    def __init__(self, argstring: str, nm: int = 16, proc: int = 0, nproc: int = 1, comm: Comm = None):
+        """proc / nproc / comm: this process's place in a process group (the
+        counterpart of the reference's MPI world); with --nproc_x / --nproc_y
+        the problem is then this process's subdomain of the global one
+        (runner.c:95-106)."""
         L = lib()
         self.env = Env()
         L.Env_initialize(ctypes.byref(self.env), 0, None)
+        self._comm = comm
+        if nproc > 1 or comm is not None:
+            _check(L.msb_env_set_comm(ctypes.byref(self.env), proc, nproc,
+                                      ctypes.byref(comm) if comm is not None else None))
         self.args = Arguments()
         L.Arguments_create_from_string(ctypes.byref(self.args), argstring.encode())
         L.Env_set_values(ctypes.byref(self.env), ctypes.byref(self.args))
         g = lambda name, d: L.Arguments_consume_int_or_default(ctypes.byref(self.args), name.encode(), d)
-        self.dims = Dimensions(g("--ncell_x", 5), g("--ncell_y", 5), g("--ncell_z", 5), g("--ne", 30), nm,
-                               g("--na", 33))
+        gx, gy = g("--ncell_x", 5), g("--ncell_y", 5)
+        npx, npy = self.env.nproc_x_, self.env.nproc_y_
+        self.x0, nx = local_extent(gx, npx, proc % npx)
+        self.y0, ny = local_extent(gy, npy, proc // npx)
+        self.dims = Dimensions(nx, ny, g("--ncell_z", 5), g("--ne", 30), nm, g("--na", 33))
+        self.dims_global = Dimensions(gx, gy, self.dims.ncell_z, self.dims.ne, nm, self.dims.na)
         self.niterations = g("--niterations", 1)
         self.quan = Quantities()
         L.Quantities_create(ctypes.byref(self.quan), self.dims, ctypes.byref(self.env))
@@ -320,6 +437,39 @@ class Problem:
 
     def set_timeout_ns(self, ns: int) -> None:
         _check(lib().Sweeper_set_spin_limit(ctypes.byref(self.sweeper), ns))
+
+    # ---------------------------------------------- decomposed sweep by steps
+    def kba_info(self):
+        """(steps per sweep, bytes of an x-face message, of a y-face message)."""
+        n, bx, by = ctypes.c_int(), ctypes.c_size_t(), ctypes.c_size_t()
+        _check(lib().msb_kba_info(ctypes.byref(self.sweeper), ctypes.byref(n), ctypes.byref(bx), ctypes.byref(by)))
+        return n.value, bx.value, by.value
+
+    def kba_set_buffers(self, send_x, send_y, recv_x_lo, recv_x_hi, recv_y_lo, recv_y_hi) -> None:
+        """Device addresses of the message buffers (None: the sweeper's own)."""
+        b = [ctypes.c_void_p(p) if p else None for p in (send_x, send_y, recv_x_lo, recv_x_hi, recv_y_lo,
+                                                          recv_y_hi)]
+        _check(lib().msb_kba_set_buffers(ctypes.byref(self.sweeper), *b))
+
+    def kba_begin(self, vo_ptr: int, vi_ptr: int) -> None:
+        _check(lib().msb_kba_begin(ctypes.byref(self.sweeper), ctypes.c_void_p(vo_ptr), ctypes.c_void_p(vi_ptr),
+                                   ctypes.byref(self.quan), ctypes.byref(self.env)))
+
+    def kba_step(self, step: int) -> None:
+        _check(lib().msb_kba_step(ctypes.byref(self.sweeper), step, ctypes.byref(self.env)))
+
+    def kba_messages(self, step: int):
+        msgs = (KbaMsg * 8)()
+        n = lib().msb_kba_messages(ctypes.byref(self.sweeper), step, msgs, 8)
+        if n < 0:
+            raise SweepError(n, last_error())
+        return [msgs[i] for i in range(n)]
+
+    def kba_unpack(self, step: int) -> None:
+        _check(lib().msb_kba_unpack(ctypes.byref(self.sweeper), step, ctypes.byref(self.env)))
+
+    def kba_end(self) -> None:
+        _check(lib().msb_kba_end(ctypes.byref(self.sweeper), ctypes.byref(self.env)))
 
     def close(self) -> None:
         if getattr(self, "_closed", True):

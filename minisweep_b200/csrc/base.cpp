@@ -6,7 +6,7 @@
 // Reference behaviour followed (file:line in olcf/minisweep):
 //   Insist message/exit           src/1_base/env_assert.c:27-32
 //   Arguments parsing             src/1_base/arguments.c:37-198
-//   Env (no MPI, 1x1 grid)        src/1_base/env_mpi.c (the #else branches)
+//   Env (process grid, group)     src/1_base/env_mpi.c:100-480
 //   --is_using_device             src/1_base/env_cuda.c:84-92
 //   Pointer                       src/1_base/pointer.c:36-267
 //   Dimensions sizes              src/2_sweeper_base/dimensions.c:36-101
@@ -21,6 +21,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "internal.h"
 
@@ -157,21 +158,43 @@ extern "C" void Env_initialize(Env* env, int argc, char** argv) {
   env->stream_kernel_faces_ = (Stream_t)s;
 }
 
+extern "C" int msb_env_set_comm(Env* env, int proc, int nproc, const msb_comm* comm) {
+  if (!env || nproc < 1 || proc < 0 || proc >= nproc)
+    return msb::set_error(MSB_ERR_ARG, "msb_env_set_comm: proc %d of %d", proc, nproc);
+  if (nproc > 1 && (!comm || !comm->exchange || !comm->sum_double || !comm->allgather_int || !comm->barrier))
+    return msb::set_error(MSB_ERR_ARG, "msb_env_set_comm: a group of %d processes needs every callback", nproc);
+  env->proc_ = proc;
+  env->nproc_world_ = nproc;
+  env->comm_ = nproc > 1 ? comm : nullptr;
+  return MSB_OK;
+}
+
+static int nproc_world(const Env* env) { return env->nproc_world_ > 0 ? env->nproc_world_ : 1; }
+
 extern "C" void Env_set_values(Env* env, Arguments* args) {
-  // env_mpi.c:114-117: only a 1 x 1 process grid is meaningful on one GPU
+  // env_mpi.c:114-135: the requested grid must fit the processes there are;
+  // process numbers beyond it are inactive.
   const int npx = Arguments_consume_int_or_default(args, "--nproc_x", 1);
   const int npy = Arguments_consume_int_or_default(args, "--nproc_y", 1);
   Insist(npx > 0 ? "Invalid nproc_x supplied." : 0);
   Insist(npy > 0 ? "Invalid nproc_y supplied." : 0);
-  Insist(npx * npy == 1 ? "This build runs one process per GPU: nproc_x = nproc_y = 1." : 0);
+  const int requested = npx * npy, world = nproc_world(env);
+  Insist(requested <= world ? "Not enough processors available." : 0);
   env->nproc_x_ = npx;
   env->nproc_y_ = npy;
-  env->is_proc_active_ = Bool_true;
+  env->is_proc_active_ = env->proc_ < requested ? Bool_true : Bool_false;
+  env->tag_ = 0;
   // env_cuda.c:87-92
   env->is_using_device_ = Arguments_consume_int_or_default(args, "--is_using_device", 0);
   Insist(env->is_using_device_ == 0 || env->is_using_device_ == 1
              ? "Invalid setting for is_using_device."
              : 0);
+}
+
+// The group's callbacks serve a decomposed grid only: a 1 x 1 run is process
+// 0 alone and talks to nobody.
+static const msb_comm* grid_comm(const Env* env) {
+  return env && env->comm_ && env->nproc_x_ * env->nproc_y_ > 1 ? env->comm_ : nullptr;
 }
 
 extern "C" void Env_finalize(Env* env) {
@@ -189,27 +212,36 @@ extern "C" Timer Env_get_time(Env* env) {
 }
 
 extern "C" Timer Env_get_synced_time(Env* env) {
-  // The reference barriers its ranks here (env.c:81-85); on one GPU the
-  // equivalent is to drain the device work queued on the Env's stream.
+  // The reference barriers its ranks here (env.c:81-85): drain the device
+  // work queued on the Env's stream, then the group's barrier.
   if (env && env->stream_kernel_faces_) cudaStreamSynchronize((cudaStream_t)env->stream_kernel_faces_);
+  Env_mpi_barrier(env);
   return Env_get_time(env);
 }
 
 extern "C" int Env_nproc_x(const Env* env) { return env->nproc_x_ > 0 ? env->nproc_x_ : 1; }
 extern "C" int Env_nproc_y(const Env* env) { return env->nproc_y_ > 0 ? env->nproc_y_ : 1; }
 extern "C" int Env_nproc(const Env* env) { return Env_nproc_x(env) * Env_nproc_y(env); }
-extern "C" Bool_t Env_is_proc_active(const Env* env) { (void)env; return Bool_true; }
+extern "C" Bool_t Env_is_proc_active(const Env* env) { return env->is_proc_active_ ? Bool_true : Bool_false; }
 extern "C" int Env_tag(const Env* env) { return env->tag_; }
 extern "C" void Env_increment_tag(Env* env, int value) { env->tag_ += value; }
 extern "C" int Env_proc(const Env* env, int proc_x, int proc_y) { return proc_x + Env_nproc_x(env) * proc_y; }
 extern "C" int Env_proc_x(const Env* env, int proc) { return proc % Env_nproc_x(env); }
 extern "C" int Env_proc_y(const Env* env, int proc) { return proc / Env_nproc_x(env); }
-extern "C" int Env_proc_this(const Env* env) { (void)env; return 0; }
+extern "C" int Env_proc_this(const Env* env) { return env->proc_; }
 extern "C" int Env_proc_x_this(const Env* env) { return Env_proc_x(env, Env_proc_this(env)); }
 extern "C" int Env_proc_y_this(const Env* env) { return Env_proc_y(env, Env_proc_this(env)); }
-extern "C" void Env_mpi_barrier(Env* env) { (void)env; }
-extern "C" double Env_sum_d(Env* env, double value) { (void)env; return value; }
-extern "C" P Env_sum_P(Env* env, P value) { (void)env; return value; }
+extern "C" void Env_mpi_barrier(Env* env) {
+  const msb_comm* c = grid_comm(env);
+  if (c) Insist(c->barrier(c->ctx, Env_nproc(env)) == 0 ? "barrier failed." : 0);
+}
+extern "C" double Env_sum_d(Env* env, double value) {
+  // env_mpi.c:309-323: a sum over the active processes
+  const msb_comm* c = grid_comm(env);
+  if (c) Insist(c->sum_double(c->ctx, Env_nproc(env), &value) == 0 ? "sum over processes failed." : 0);
+  return value;
+}
+extern "C" P Env_sum_P(Env* env, P value) { return Env_sum_d(env, value); }
 extern "C" Bool_t Env_cuda_is_using_device(const Env* const env) { return env->is_using_device_; }
 extern "C" Bool_t Env_cuda_last_call_succeeded(void) { return cudaPeekAtLastError() == cudaSuccess; }
 extern "C" Stream_t Env_cuda_stream_kernel_faces(Env* env) { return env->stream_kernel_faces_; }
@@ -411,19 +443,32 @@ extern "C" void Quantities_init_am_matrices_(Quantities* quan, const Dimensions 
 }
 
 extern "C" void Quantities_init_decomp_(Quantities* quan, const Dimensions dims, Env* env) {
-  // quantities_testing_c.h:206-333 on a 1 x 1 process grid: bases 0, global
-  // sizes equal to the local ones.
+  // quantities_testing_c.h:206-333: the offsets of this process's subdomain
+  // from the local x (y) sizes of the processes in its row (column).  The
+  // reference gathers them with point-to-point messages; here one allgather.
+  const int npx = Env_nproc_x(env), npy = Env_nproc_y(env), nproc = npx * npy;
+  const int px = Env_proc_x_this(env), py = Env_proc_y_this(env);
   quan->ncell_z_g = dims.ncell_z;
-  quan->ix_base_vals = malloc_host_int(Env_nproc_x(env) + 1);
-  quan->iy_base_vals = malloc_host_int(Env_nproc_y(env) + 1);
+  quan->ix_base_vals = malloc_host_int(npx + 1);
+  quan->iy_base_vals = malloc_host_int(npy + 1);
   quan->ix_base_vals[0] = 0;
-  quan->ix_base_vals[1] = dims.ncell_x;
   quan->iy_base_vals[0] = 0;
-  quan->iy_base_vals[1] = dims.ncell_y;
-  quan->ix_base = 0;
-  quan->iy_base = 0;
-  quan->ncell_x_g = dims.ncell_x;
-  quan->ncell_y_g = dims.ncell_y;
+  if (nproc == 1) {
+    quan->ix_base_vals[1] = dims.ncell_x;
+    quan->iy_base_vals[1] = dims.ncell_y;
+  } else {
+    const msb_comm* c = grid_comm(env);
+    Insist(c ? "A decomposed grid needs the Env's process group (msb_env_set_comm)." : 0);
+    std::vector<int> nx(nproc), ny(nproc);
+    Insist(c->allgather_int(c->ctx, nproc, dims.ncell_x, nx.data()) == 0 ? "allgather failed." : 0);
+    Insist(c->allgather_int(c->ctx, nproc, dims.ncell_y, ny.data()) == 0 ? "allgather failed." : 0);
+    for (int i = 0; i < npx; ++i) quan->ix_base_vals[1 + i] = quan->ix_base_vals[i] + nx[Env_proc(env, i, py)];
+    for (int i = 0; i < npy; ++i) quan->iy_base_vals[1 + i] = quan->iy_base_vals[i] + ny[Env_proc(env, px, i)];
+  }
+  quan->ix_base = quan->ix_base_vals[px];
+  quan->iy_base = quan->iy_base_vals[py];
+  quan->ncell_x_g = quan->ix_base_vals[npx];
+  quan->ncell_y_g = quan->iy_base_vals[npy];
 }
 
 extern "C" void Quantities_create(Quantities* quan, const Dimensions dims, Env* env) {

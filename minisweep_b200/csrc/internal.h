@@ -78,4 +78,40 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
 // about `window` tasks.
 int pick_gp_block(int nx, int ny, int ngp, int tx, int ty, int window);
 
+// ------------------------------------------------------- KBA decomposition
+// One slab of a decomposed sweep: one octant over the process's whole x-y
+// extent and the z-planes [z0, z1).  The edge flags say where the slab's
+// faces come from and go: *_in on an x/y edge = the neighbouring process's
+// face, placed in the face plane before the launch; z_in = the previous
+// z-block's face, left in the plane by an earlier launch; *_out = somebody
+// reads the face leaving that side; first = the slab's cells get vo = (not +=).
+struct SlabEdges {
+  bool x_in = false, x_out = false, y_in = false, y_out = false, z_in = false, z_out = false, first = false;
+};
+// Tasks of one slab in launch order (block of group pairs, tile level, group
+// pair, tile); dependencies only between tiles of the slab.
+int build_slab_schedule(int nx, int ny, int z0, int z1, int ngp, int tx, int ty, int gp_block, int oct,
+                        const SlabEdges& e, Schedule& out);
+int pick_gp_block_slab(int nx, int ny, int ngp, int tx, int ty, int window);
+
+// Steps of a decomposed sweep: unit k = (unit_oct[k], unit_zb[k]) is swept by
+// process p = px + nproc_x * py at step start[p * nunit + k].
+struct KbaPlan {
+  int npx = 1, npy = 1, nblock = 1, nstep = 0;
+  std::vector<int> unit_oct, unit_zb, start;
+  int nunit() const { return (int)unit_oct.size(); }
+  int at(int px, int py, int k) const { return start[(size_t)(px + npx * py) * nunit() + k]; }
+};
+// A face slab crossing between neighbours after a step: is_send 1 = this
+// process sends unit `unit`'s leaving face to `peer`; 0 = it receives the
+// face entering its own copy of that unit.  axis 0: x faces (yz planes),
+// 1: y faces (xz planes).  side: the peer's position along the axis (0 the
+// lower neighbour, 1 the higher).
+struct KbaMsg {
+  int peer, is_send, axis, side, unit;
+};
+int build_kba_plan(int npx, int npy, int nblock, KbaPlan& out);
+int kba_unit_at(const KbaPlan& plan, int proc, int step);  // unit swept at the step, or -1
+int kba_messages(const KbaPlan& plan, int proc, int step, std::vector<KbaMsg>& msgs);
+
 }  // namespace msb

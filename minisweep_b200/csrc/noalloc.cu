@@ -277,7 +277,7 @@ extern "C" int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double*
   }
   if ((rc = cuda_check(cudaMemsetAsync(sync, 0, sync_b, st), "clear progress"))) return rc;
 
-  Fp64Params P;
+  Fp64Params P{};
   P.pr.vi = vi_d;
   P.pr.vo = vo_d;
   P.pr.afm = a_from_m_d;

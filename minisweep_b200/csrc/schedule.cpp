@@ -178,6 +178,80 @@ int build_schedule(int nx, int ny, int nz, int ngp, int tx, int ty, int gp_block
   return MSB_OK;
 }
 
+int build_slab_schedule(int nx, int ny, int z0, int z1, int ngp, int tx, int ty, int gp_block, int oct,
+                        const SlabEdges& e, Schedule& out) {
+  if (nx <= 0 || ny <= 0 || z1 <= z0 || z0 < 0 || ngp <= 0 || tx <= 0 || ty <= 0 || gp_block <= 0 || oct < 0 ||
+      oct >= NOCTANT)
+    return set_error(MSB_ERR_ARG, "slab schedule: invalid sizes");
+  const int ntx = ceil_div(nx, tx), nty = ceil_div(ny, ty);
+  if ((long long)ntx * nty * ngp >= (1LL << 30)) return set_error(MSB_ERR_ARG, "slab schedule: too many tasks");
+  out = Schedule();
+  out.nx = nx;
+  out.ny = ny;
+  out.nz = z1;
+  out.ngp = ngp;
+  out.tx = tx;
+  out.ty = ty;
+  const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1;
+  std::vector<int> index((size_t)ngp * ntx * nty, -1);
+  auto dense = [&](int gp, int itx, int ity) { return ((size_t)gp * ntx + itx) * nty + ity; };
+  std::vector<int>& rec = out.rec;
+  rec.reserve((size_t)ngp * ntx * nty * MSB_TASK_INTS);
+  int n = 0;
+  for (int gb = 0; gb * gp_block < ngp; ++gb)
+    for (int level = 0; level < ntx + nty - 1; ++level)
+      for (int gp = gb * gp_block; gp < std::min(ngp, (gb + 1) * gp_block); ++gp)
+        for (int ity = 0; ity < nty; ++ity) {
+          // ax, ay: the tile's position counted from the slab's upwind corner
+          const int ay = dy > 0 ? ity : nty - 1 - ity;
+          const int ax = level - ay;
+          if (ax < 0 || ax >= ntx) continue;
+          const int itx = dx > 0 ? ax : ntx - 1 - ax;
+          rec.resize(rec.size() + MSB_TASK_INTS, -1);
+          int* r = &rec[(size_t)n * MSB_TASK_INTS];
+          r[TK_OCT] = oct;
+          r[TK_PHASE] = 0;
+          r[TK_GP] = gp;
+          r[TK_X0] = itx * tx;
+          r[TK_X1] = std::min(nx, (itx + 1) * tx);
+          r[TK_Y0] = ity * ty;
+          r[TK_Y1] = std::min(ny, (ity + 1) * ty);
+          r[TK_Z0] = z0;
+          r[TK_Z1] = z1;
+          r[TK_LEVEL] = level;
+          int flags = 0, mode = 0;
+          if (ax > 0) {
+            r[TK_DEP_X] = index[dense(gp, itx - dx, ity)];
+            mode |= DM_X_PLANE;
+          }
+          if (ay > 0) {
+            r[TK_DEP_Y] = index[dense(gp, itx, ity - dy)];
+            mode |= DM_Y_PLANE;
+          }
+          if (ax > 0 || e.x_in) flags |= TF_X_IN;
+          if (ax < ntx - 1 || e.x_out) flags |= TF_X_OUT;
+          if (ay > 0 || e.y_in) flags |= TF_Y_IN;
+          if (ay < nty - 1 || e.y_out) flags |= TF_Y_OUT;
+          if (e.z_in) flags |= TF_Z_IN;
+          if (e.z_out) flags |= TF_Z_OUT;
+          if (e.first) flags |= TF_FIRST;
+          r[TK_FLAGS] = flags;
+          r[TK_DEP_MODE] = mode;
+          index[dense(gp, itx, ity)] = n;
+          if ((mode & DM_X_PLANE && r[TK_DEP_X] < 0) || (mode & DM_Y_PLANE && r[TK_DEP_Y] < 0))
+            return set_error(MSB_ERR_ARG, "slab schedule: dependency not topological");
+          ++n;
+        }
+  return MSB_OK;
+}
+
+int pick_gp_block_slab(int nx, int ny, int ngp, int tx, int ty, int window) {
+  const int ntx = ceil_div(nx, tx), nty = ceil_div(ny, ty);
+  const double per_level = (double)ntx * nty / (ntx + nty - 1);
+  int b = (int)((window + per_level - 1) / per_level);
+  return std::max(1, std::min(b, ngp));
+}
+
 int pick_gp_block(int nx, int ny, int ngp, int tx, int ty, int window) {
   // one region sweep: ntx x nty tiles over ntx + nty - 1 levels, 8 octants
   const int hx = (nx + 1) / 2, hy = (ny + 1) / 2;

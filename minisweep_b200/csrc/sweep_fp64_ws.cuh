@@ -60,8 +60,11 @@ struct Fp64Prob {
   int nx, ny, nz, ne, na, ngp;
   int ia_base;  // angle index of the first angle of afm / mfa (a multiple of 64: passes over na > 64)
   int ie_base;  // global index of group 0 (energy-group slices of a larger problem)
-  int vo_add;   // nonzero: every phase adds to vo (the passes after the first)
-  int l2_hints; // nonzero: faces written evict_last, state and consumed faces evict_first (chained kernel)
+  signed char vo_add;    // nonzero: every phase adds to vo (the passes after the first)
+  signed char l2_hints;  // nonzero: faces written evict_last, state and consumed faces evict_first (chained kernel)
+  signed char sp_off;    // (ix_base + 3 iy_base) & 3 of a process's subdomain (KBA decomposition): the space
+                         // factor (quantities_testing_kernels.h:97-126) takes global coordinates
+  signed char pad_;
 };
 
 // One problem per launch.
@@ -546,7 +549,7 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
     // exact small integers, so the per-lane factor is formed once per task
     const double face_k =
         gval ? (double)d_scale_energy(Q.ie_base + g_col) * (double)d_scale_unknown(q & 3) * so : 0.0;
-    const int sp_xy = ix + 3 * iy + 2;  // log2 s_space(x, y, z) = (sp_xy + 7 z) & 3
+    const int sp_xy = ix + 3 * iy + 2 + Q.sp_off;  // log2 s_space(x, y, z) = (sp_xy + 7 z) & 3
     // state offsets (doubles) of this column: + zstep per plane
     const size_t col = (size_t)NM_ * NU * (ix + (size_t)Q.nx * iy);
     const long long zstep = (long long)slab * Q.ne * dz;
@@ -686,7 +689,7 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int ia = 32 * ch + 8 * t + 2 * r + i, iag = Q.ia_base + ia;
-                fyz[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(gx, iy, iz)) * face_k : 0.0;
+                fyz[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(gx + Q.sp_off, iy, iz)) * face_k : 0.0;
               }
             }
             if (in_xz) {
@@ -699,7 +702,7 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int ia = 32 * ch + 8 * t + 2 * r + i, iag = Q.ia_base + ia;
-                fxz[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(ix, gy, iz)) * face_k : 0.0;
+                fxz[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(ix + Q.sp_off, gy, iz)) * face_k : 0.0;
               }
             }
             if (c > 0) {
@@ -714,7 +717,7 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
 #pragma unroll
               for (int i = 0; i < 2; ++i) {
                 const int ia = 32 * ch + 8 * t + 2 * r + i, iag = Q.ia_base + ia;
-                fxy[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(ix, iy, gz)) * face_k : 0.0;
+                fxy[i] = ia < Q.na ? (double)((1 + iag) << (iag & 7)) * d_pow2(d_log2_space(ix + Q.sp_off, iy, gz)) * face_k : 0.0;
               }
             }
 

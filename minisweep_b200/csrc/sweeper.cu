@@ -13,6 +13,7 @@
 #include <memory>
 #include <new>
 #include <type_traits>
+#include <vector>
 
 #include "internal.h"
 #include "sweep_fp64_chain.cuh"
@@ -212,6 +213,31 @@ struct AltPlan {
   float ms = 0.f;  // its autotuning sweep
 };
 
+// A decomposed sweep (--nproc_x * --nproc_y > 1): this process's units, one
+// slab schedule each, and the message buffers.  Unit k's tasks are
+// d_tasks[off[k] .. off[k] + cnt[k]) with slab-local dependencies.
+struct KbaState {
+  KbaPlan plan;
+  int proc = 0, px = 0, py = 0, nzb = 0, npass = 1, pa = 64;
+  std::vector<long long> off, cnt;
+  std::vector<int> grid;
+  int* d_tasks = nullptr;
+  long long ntask_max = 0;
+  size_t plane_pass[3] = {0, 0, 0};  // bytes of one angle pass's plane: xy, xz, yz
+  size_t slab_bytes[2] = {0, 0};     // one pass's face slab of a unit: x faces, y faces
+  // message buffers: send x, send y, receive x from lower / higher, y lower / higher
+  void* buf[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  void* own[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  double* vo_d = nullptr;
+  const double* vi_d = nullptr;
+  int rc = 0;  // first error of the sweep in progress (later steps still exchange)
+  size_t msg_bytes(int axis) const { return (size_t)npass * slab_bytes[axis]; }
+  ~KbaState() {
+    cudaFree(d_tasks);
+    for (void* p : own) cudaFree(p);
+  }
+};
+
 struct SweeperImpl {
   Dimensions dims{};
   int precision = 0;
@@ -246,6 +272,8 @@ struct SweeperImpl {
   int ie_base = 0;                // --ie_base: global index of this sweeper's group 0
   int window = 4;                 // --task_window: tasks between a tile and its downwind neighbour, x SMs
   int l2_hints = 0;               // --l2_hints: L2 eviction policies in the chained FP64 kernel
+  int sp_off = 0;                 // (ix_base + 3 iy_base) & 3 of a decomposed process's subdomain
+  std::unique_ptr<KbaState> kba;  // set: the sweep is decomposed over a process grid
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
@@ -376,13 +404,16 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
 
 // The columns a0 .. a0 + nac of a_from_m[oct][im][ia] and the rows of
 // m_from_a[oct][ia][im] into the pass buffers (layouts of an na = nac problem).
-static int copy_pass_matrices(SweeperImpl& S, int a0, int nac, cudaStream_t stream) {
+static int copy_pass_matrices(SweeperImpl& S, int a0, int nac, cudaStream_t stream, double* dst_a = nullptr,
+                              double* dst_m = nullptr) {
   const int na = S.dims.na, nm = S.dims.nm;
-  int rc = cuda_check(cudaMemcpy2DAsync(S.d_afm_c, nac * sizeof(double), S.d_afm + a0, na * sizeof(double),
+  if (!dst_a) dst_a = S.d_afm_c;
+  if (!dst_m) dst_m = S.d_mfa_c;
+  int rc = cuda_check(cudaMemcpy2DAsync(dst_a, nac * sizeof(double), S.d_afm + a0, na * sizeof(double),
                                         nac * sizeof(double), (size_t)nm * NOCTANT, cudaMemcpyDeviceToDevice, stream),
                       "a_from_m pass");
   if (rc) return rc;
-  return cuda_check(cudaMemcpy2DAsync(S.d_mfa_c, (size_t)nac * nm * sizeof(double), S.d_mfa + (size_t)a0 * nm,
+  return cuda_check(cudaMemcpy2DAsync(dst_m, (size_t)nac * nm * sizeof(double), S.d_mfa + (size_t)a0 * nm,
                                       (size_t)na * nm * sizeof(double), (size_t)nac * nm * sizeof(double), NOCTANT,
                                       cudaMemcpyDeviceToDevice, stream),
                     "m_from_a pass");
@@ -415,7 +446,10 @@ static void fill_params(const SweeperImpl& S, X& x, PP& P, const double* vi_d, c
   x.ngp = S.ngp;
   x.ia_base = 0;
   x.ie_base = S.ie_base;
-  if constexpr (std::is_same<X, Fp64Prob>::value) x.l2_hints = S.l2_hints;
+  if constexpr (std::is_same<X, Fp64Prob>::value) {
+    x.l2_hints = S.l2_hints;
+    x.sp_off = S.sp_off;
+  }
   P.tasks = d_tasks;
   P.ntask = ntask;
   P.sy.sync = S.d_sync;
@@ -488,10 +522,10 @@ static void swap_plan(SweeperImpl& S, AltPlan& a) {
 
 static int impl_sync(SweeperImpl& S, cudaStream_t stream);
 
-// Launches one sweep: vo_d = sweep(vi_d), asynchronously on `stream` (the
-// first sweep of an autotuning sweeper waits for the stream).
-static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
-                      const double* afm_d, const double* mfa_d, cudaStream_t stream) {
+// The sweep's transform matrices into the sweeper's device buffers, from the
+// device copies when there are some, else from the host.
+static int load_matrices(SweeperImpl& S, const double* afm_h, const double* mfa_h, const double* afm_d,
+                         const double* mfa_d, cudaStream_t stream) {
   int rc;
   const size_t nmat = (size_t)S.dims.nm * S.dims.na * NOCTANT;
   if (afm_d && mfa_d) {
@@ -509,6 +543,15 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
                          "copy m_from_a")))
       return rc;
   }
+  return MSB_OK;
+}
+
+// Launches one sweep: vo_d = sweep(vi_d), asynchronously on `stream` (the
+// first sweep of an autotuning sweeper waits for the stream).
+static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
+                      const double* afm_d, const double* mfa_d, cudaStream_t stream) {
+  int rc;
+  if ((rc = load_matrices(S, afm_h, mfa_h, afm_d, mfa_d, stream))) return rc;
   if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
   if (S.var.fn && S.autotune && !S.tuned) {
     // First sweep of an autotuning sweeper: the same sweep with the sweeper's
@@ -582,6 +625,276 @@ static int impl_sync(SweeperImpl& S, cudaStream_t stream) {
     return set_error(MSB_ERR_TIMEOUT, "a device wait ran out of time (task %d); sweep aborted", S.h_status[SY_ERRTASK]);
   if (err) return set_error(err, "device error %d", err);
   return MSB_OK;
+}
+
+// ------------------------------------------------------- KBA decomposition
+// Process `proc` of an npx x npy grid sweeps its subdomain with the staged
+// FP64 kernel, one launch per (octant, z-block) unit.  The face planes hold
+// one region per angle pass so that a unit's passes leave each other's
+// faces intact until they are sent.
+static int impl_create_kba(SweeperImpl& S, const Dimensions& dims, int tile, int nblock, int npx, int npy, int proc,
+                           int sp_off) {
+  S.dims = dims;
+  S.precision = 0;
+  S.sp_off = sp_off & 3;
+  S.var = pick_variant(dims.nm, dims.na, 0, tile, 0);
+  if (!S.var.valid())
+    return set_error(MSB_ERR_UNSUPPORTED, "no kernel variant for nm=%d na=%d (nm in {4,8,16}; na <= 128)", dims.nm,
+                     dims.na);
+  S.ngp = (dims.ne + 1) / 2;
+  const Variant& var = S.var;
+  int rc, dev = 0, nsm = 0, occ = 0;
+  if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+  if ((rc = cuda_check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count"))) return rc;
+  S.nsm = nsm;
+  if ((rc = cuda_check(cudaFuncSetAttribute(var.func(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)var.smem),
+                       "cudaFuncSetAttribute")))
+    return rc;
+  if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, var.func(), var.threads, var.smem),
+                       "occupancy")))
+    return rc;
+  if (occ < 1) return set_error(MSB_ERR_UNSUPPORTED, "sweep kernel does not fit on an SM");
+
+  std::unique_ptr<KbaState> K(new (std::nothrow) KbaState());
+  if (!K) return set_error(MSB_ERR_ARG, "out of host memory");
+  if ((rc = build_kba_plan(npx, npy, nblock, K->plan))) return rc;
+  K->proc = proc;
+  K->px = proc % npx;
+  K->py = proc / npx;
+  K->nzb = dims.ncell_z / nblock;
+  K->pa = var.pass;
+  K->npass = (dims.na + var.pass - 1) / var.pass;
+  const int nunit = K->plan.nunit(), nx = dims.ncell_x, ny = dims.ncell_y, nz = dims.ncell_z;
+  S.gp_block = pick_gp_block_slab(nx, ny, S.ngp, var.tx, var.ty, S.window * nsm);
+  K->off.resize(nunit);
+  K->cnt.resize(nunit);
+  K->grid.resize(nunit);
+  std::vector<int>& all = S.sched.rec;  // every unit's tasks, for Sweeper_debug_tasks
+  all.clear();
+  for (int k = 0; k < nunit; ++k) {
+    const int oct = K->plan.unit_oct[k], zb = K->plan.unit_zb[k];
+    const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1, dz = (oct & 4) ? -1 : 1;
+    SlabEdges e;
+    e.x_in = K->px - dx >= 0 && K->px - dx < npx;
+    e.x_out = K->px + dx >= 0 && K->px + dx < npx;
+    e.y_in = K->py - dy >= 0 && K->py - dy < npy;
+    e.y_out = K->py + dy >= 0 && K->py + dy < npy;
+    e.z_in = dz > 0 ? zb > 0 : zb < nblock - 1;
+    e.z_out = dz > 0 ? zb < nblock - 1 : zb > 0;
+    e.first = k < nblock;  // the first octant of the sequence visits every z-block first
+    Schedule sch;
+    if ((rc = build_slab_schedule(nx, ny, zb * K->nzb, (zb + 1) * K->nzb, S.ngp, var.tx, var.ty, S.gp_block, oct, e,
+                                  sch)))
+      return rc;
+    K->off[k] = (long long)(all.size() / MSB_TASK_INTS);
+    K->cnt[k] = sch.ntask();
+    K->grid[k] = (int)std::min<long long>(sch.ntask(), (long long)nsm * occ);
+    K->ntask_max = std::max(K->ntask_max, sch.ntask());
+    all.insert(all.end(), sch.rec.begin(), sch.rec.end());
+  }
+  S.sched.nx = nx;
+  S.sched.ny = ny;
+  S.sched.nz = nz;
+  S.sched.ngp = S.ngp;
+  S.sched.tx = var.tx;
+  S.sched.ty = var.ty;
+  if (K->ntask_max >= (1LL << 31) - SY_PROGRESS) return set_error(MSB_ERR_ARG, "too many tasks");
+  if ((rc = cuda_check(cudaMalloc(&K->d_tasks, all.size() * sizeof(int)), "cudaMalloc tasks"))) return rc;
+  if ((rc = cuda_check(cudaMemcpy(K->d_tasks, all.data(), all.size() * sizeof(int), cudaMemcpyHostToDevice),
+                       "copy tasks")))
+    return rc;
+  S.sync_ints = SY_PROGRESS + (size_t)K->ntask_max;
+  if ((rc = cuda_check(cudaMalloc(&S.d_sync, S.sync_ints * sizeof(int)), "cudaMalloc sync"))) return rc;
+  if ((rc = cuda_check(cudaMallocHost(&S.h_status, 8 * sizeof(int)), "cudaMallocHost status"))) return rc;
+  const size_t E = var.entry_bytes, per = (size_t)NOCTANT * S.ngp * E;
+  K->plane_pass[0] = per * ny * nx;
+  K->plane_pass[1] = per * nz * nx;
+  K->plane_pass[2] = per * nz * ny;
+  for (int f = 0; f < 3; ++f) {
+    S.face_bytes[f] = K->plane_pass[f] * K->npass;
+    if ((rc = cuda_check(cudaMalloc(&S.d_face[f], S.face_bytes[f]), "cudaMalloc faces"))) return rc;
+  }
+  K->slab_bytes[0] = (size_t)S.ngp * K->nzb * ny * E;
+  K->slab_bytes[1] = (size_t)S.ngp * K->nzb * nx * E;
+  const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
+  if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
+  if ((rc = cuda_check(cudaMalloc(&S.d_mfa, nmat * sizeof(double)), "cudaMalloc m_from_a"))) return rc;
+  if (K->npass > 1) {
+    const size_t blk = (size_t)dims.nm * K->pa * NOCTANT * K->npass;
+    if ((rc = cuda_check(cudaMalloc(&S.d_afm_c, blk * sizeof(double)), "cudaMalloc a_from_m passes"))) return rc;
+    if ((rc = cuda_check(cudaMalloc(&S.d_mfa_c, blk * sizeof(double)), "cudaMalloc m_from_a passes"))) return rc;
+  }
+  S.kba = std::move(K);
+  return MSB_OK;
+}
+
+// Face rows of one unit's slab in one pass's plane: x faces (axis 0) are the
+// yz plane's rows [oct][gp][z-block][all y], y faces the xz plane's
+// [oct][gp][z-block][all x]; one row run per group pair, `pitch` apart.
+static char* kba_rows(const SweeperImpl& S, int axis, int pass, int unit, size_t& pitch, size_t& width) {
+  const KbaState& K = *S.kba;
+  const size_t E = S.var.entry_bytes;
+  const int n_in = axis == 0 ? S.dims.ncell_y : S.dims.ncell_x, f = axis == 0 ? 2 : 1;
+  pitch = (size_t)S.dims.ncell_z * n_in * E;
+  width = (size_t)K.nzb * n_in * E;
+  const int oct = K.plan.unit_oct[unit], zb = K.plan.unit_zb[unit];
+  return static_cast<char*>(S.d_face[f]) + pass * K.plane_pass[f] +
+         ((size_t)oct * S.ngp * S.dims.ncell_z + (size_t)zb * K.nzb) * n_in * E;
+}
+
+// Matrices of the sweep (and every pass's share of them) in place, progress
+// cleared; the steps follow.
+static int kba_begin(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
+                     const double* afm_d, const double* mfa_d, cudaStream_t stream) {
+  KbaState& K = *S.kba;
+  int rc;
+  if ((rc = load_matrices(S, afm_h, mfa_h, afm_d, mfa_d, stream))) return rc;
+  if (K.npass > 1) {
+    const size_t blk = (size_t)S.dims.nm * K.pa * NOCTANT;
+    for (int c = 0; c < K.npass; ++c) {
+      const int a0 = K.pa * c, nac = std::min(K.pa, S.dims.na - a0);
+      if ((rc = copy_pass_matrices(S, a0, nac, stream, S.d_afm_c + c * blk, S.d_mfa_c + c * blk))) return rc;
+    }
+  }
+  if ((rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), stream), "reset sync"))) return rc;
+  K.vo_d = vo_d;
+  K.vi_d = vi_d;
+  K.rc = MSB_OK;
+  S.nlaunch = 0;
+  return MSB_OK;
+}
+
+// This process's unit of `step` (every pass), then its leaving faces into the
+// send buffers; waits for the device.  After an error the later steps launch
+// nothing, so that the process still takes part in every exchange.
+static int kba_step(SweeperImpl& S, int step, cudaStream_t stream) {
+  KbaState& K = *S.kba;
+  if (K.rc) return K.rc;
+  const int k = kba_unit_at(K.plan, K.proc, step);
+  if (k < 0) return MSB_OK;
+  const int oct = K.plan.unit_oct[k];
+  int rc = MSB_OK;
+  for (int c = 0; c < K.npass && !rc; ++c) {
+    rc = cuda_check(cudaMemsetAsync(S.d_sync + SY_COUNTER, 0, sizeof(int), stream), "reset sync");
+    if (!rc)
+      rc = cuda_check(cudaMemsetAsync(S.d_sync + SY_PROGRESS, 0, (size_t)K.cnt[k] * sizeof(int), stream),
+                      "reset sync");
+    if (rc) break;
+    Fp64Params P{};
+    fill_params<double>(S, P.pr, P, K.vi_d, K.d_tasks + K.off[k] * MSB_TASK_INTS, K.cnt[k]);
+    P.pr.vo = K.vo_d;
+    P.pr.vo_add = c > 0 ? 1 : 0;
+    P.pr.fxy = reinterpret_cast<double*>(static_cast<char*>(S.d_face[0]) + c * K.plane_pass[0]);
+    P.pr.fxz = reinterpret_cast<double*>(static_cast<char*>(S.d_face[1]) + c * K.plane_pass[1]);
+    P.pr.fyz = reinterpret_cast<double*>(static_cast<char*>(S.d_face[2]) + c * K.plane_pass[2]);
+    if (K.npass > 1) {
+      const size_t blk = (size_t)S.dims.nm * K.pa * NOCTANT;
+      P.pr.afm = S.d_afm_c + c * blk;
+      P.pr.mfa = S.d_mfa_c + c * blk;
+      P.pr.na = std::min(K.pa, S.dims.na - K.pa * c);
+      P.pr.ia_base = K.pa * c;
+    }
+    S.var.fn<<<K.grid[k], S.var.threads, S.var.smem, stream>>>(P);
+    rc = cuda_check(cudaGetLastError(), "sweep kernel launch");
+    ++S.nlaunch;
+  }
+  // leaving faces of the unit for the downwind neighbours
+  const int dx = (oct & 1) ? -1 : 1, dy = (oct & 2) ? -1 : 1;
+  const bool down[2] = {K.px + dx >= 0 && K.px + dx < K.plan.npx, K.py + dy >= 0 && K.py + dy < K.plan.npy};
+  for (int axis = 0; axis < 2 && !rc; ++axis) {
+    if (!down[axis]) continue;
+    for (int c = 0; c < K.npass && !rc; ++c) {
+      size_t pitch, width;
+      const char* src = kba_rows(S, axis, c, k, pitch, width);
+      rc = cuda_check(cudaMemcpy2DAsync(static_cast<char*>(K.buf[axis]) + c * K.slab_bytes[axis], width, src, pitch,
+                                        width, S.ngp, cudaMemcpyDeviceToDevice, stream),
+                      "pack faces");
+    }
+  }
+  if (!rc)
+    rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
+                    "status copy");
+  if (!rc) rc = impl_sync(S, stream);
+  K.rc = rc;
+  return rc;
+}
+
+// The step's messages with this process's buffers.
+static int kba_message_list(const SweeperImpl& S, int step, std::vector<msb_kba_msg>& out) {
+  const KbaState& K = *S.kba;
+  std::vector<KbaMsg> msgs;
+  kba_messages(K.plan, K.proc, step, msgs);
+  out.clear();
+  for (const KbaMsg& m : msgs) {
+    msb_kba_msg r;
+    r.peer = m.peer;
+    r.is_send = m.is_send;
+    r.axis = m.axis;
+    r.side = m.side;
+    r.bytes = K.msg_bytes(m.axis);
+    r.buf = m.is_send ? K.buf[m.axis] : K.buf[2 + 2 * m.axis + m.side];
+    out.push_back(r);
+  }
+  return (int)out.size();
+}
+
+// Faces received after `step` into this process's planes (asynchronous: the
+// next step's launch follows on the same stream).
+static int kba_unpack(SweeperImpl& S, int step, cudaStream_t stream) {
+  KbaState& K = *S.kba;
+  if (K.rc) return K.rc;
+  std::vector<KbaMsg> msgs;
+  kba_messages(K.plan, K.proc, step, msgs);
+  int rc = MSB_OK;
+  for (const KbaMsg& m : msgs) {
+    if (m.is_send) continue;
+    const char* src = static_cast<const char*>(K.buf[2 + 2 * m.axis + m.side]);
+    for (int c = 0; c < K.npass && !rc; ++c) {
+      size_t pitch, width;
+      char* dst = kba_rows(S, m.axis, c, m.unit, pitch, width);
+      rc = cuda_check(cudaMemcpy2DAsync(dst, pitch, src + c * K.slab_bytes[m.axis], width, width, S.ngp,
+                                        cudaMemcpyDeviceToDevice, stream),
+                      "unpack faces");
+    }
+  }
+  K.rc = rc;
+  return rc;
+}
+
+// Message buffers the sweeper owns, for the ones the host did not provide.
+static int kba_own_buffers(SweeperImpl& S) {
+  KbaState& K = *S.kba;
+  for (int i = 0; i < 6; ++i) {
+    if (K.buf[i]) continue;
+    const size_t b = K.msg_bytes(i == 0 ? 0 : i == 1 ? 1 : (i - 2) / 2);
+    if (!K.own[i]) {
+      int rc = cuda_check(cudaMalloc(&K.own[i], b ? b : 16), "cudaMalloc message buffer");
+      if (rc) return rc;
+    }
+    K.buf[i] = K.own[i];
+  }
+  return MSB_OK;
+}
+
+// A whole decomposed sweep with the transport of the Env's process group.
+static int kba_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
+                     const double* afm_d, const double* mfa_d, const msb_comm* comm, cudaStream_t stream) {
+  KbaState& K = *S.kba;
+  if (!comm) return set_error(MSB_ERR_ARG, "a decomposed sweep needs the Env's process group (msb_env_set_comm)");
+  int rc = kba_own_buffers(S);
+  if (!rc) rc = kba_begin(S, vo_d, vi_d, afm_h, mfa_h, afm_d, mfa_d, stream);
+  if (rc) K.rc = rc;
+  std::vector<msb_kba_msg> msgs;
+  // every process takes every step's exchange, errors or not
+  for (int step = 0; step < K.plan.nstep; ++step) {
+    kba_step(S, step, stream);
+    const int n = kba_message_list(S, step, msgs);
+    if (comm->exchange(comm->ctx, msgs.data(), n) != 0 && !K.rc)
+      K.rc = set_error(MSB_ERR_ARG, "face exchange failed at step %d", step);
+    kba_unpack(S, step, stream);
+  }
+  if (!K.rc) K.rc = cuda_check(cudaStreamSynchronize(stream), "sweep");
+  return K.rc;
 }
 
 }  // namespace msb
@@ -671,14 +984,28 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // group ie_base + ie (one process per GPU, each sweeping its own groups)
   const int ie_base = Arguments_consume_int_or_default(args, "--ie_base", 0);
   if (ie_base < 0) return msb::set_error(MSB_ERR_ARG, "--ie_base must be >= 0");
-  (void)env;
 
   std::unique_ptr<SweeperImpl> S(new (std::nothrow) SweeperImpl());
   if (!S) return msb::set_error(MSB_ERR_ARG, "out of host memory");
   S->ie_base = ie_base;
   S->window = task_window;
   S->l2_hints = l2_hints;
-  const int rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0, fp64_kernel);
+  int rc;
+  if (env && Env_nproc(env) > 1) {
+    // KBA decomposition over the Env's process grid (sweeper_kba_c.h:44-287
+    // with nproc_x * nproc_y > 1): this process's subdomain, offsets from the
+    // Quantities (quantities_testing_c.h:206-333)
+    if (!quan) return msb::set_error(MSB_ERR_ARG, "a decomposed sweep needs the Quantities (subdomain offsets)");
+    if (sweeper->precision != 0 || fp64_kernel != 0 || autotune != 0)
+      return msb::set_error(MSB_ERR_UNSUPPORTED,
+                            "a decomposed sweep (--nproc_x * --nproc_y > 1) runs the staged FP64 kernel: "
+                            "--precision 0 --fp64_kernel 0 --autotune 0");
+    if (!Env_is_proc_active(env)) return msb::set_error(MSB_ERR_ARG, "this process is not in the process grid");
+    rc = msb::impl_create_kba(*S, dims, tile, sweeper->nblock_z, Env_nproc_x(env), Env_nproc_y(env),
+                              Env_proc_this(env), quan->ix_base + 3 * quan->iy_base);
+  } else {
+    rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0, fp64_kernel);
+  }
   if (rc) return rc;
   sweeper->impl_ = S.release();
   return MSB_OK;
@@ -700,6 +1027,10 @@ extern "C" int Sweeper_sweep_device(Sweeper* sweeper, double* vo_d, const double
   if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
   if (!vo_d || !vi_d || !quan) return msb::set_error(MSB_ERR_ARG, "null argument");
   const bool mats_on_dev = quan->a_from_m.d_ && quan->m_from_a.d_;
+  if (S->kba)
+    return msb::kba_sweep(*S, vo_d, vi_d, quan->a_from_m.h_, quan->m_from_a.h_,
+                          mats_on_dev ? quan->a_from_m.d_ : nullptr, mats_on_dev ? quan->m_from_a.d_ : nullptr,
+                          env ? env->comm_ : nullptr, stream_of(env));
   return msb::impl_sweep(*S, vo_d, vi_d, quan->a_from_m.h_, quan->m_from_a.h_,
                          mats_on_dev ? quan->a_from_m.d_ : nullptr, mats_on_dev ? quan->m_from_a.d_ : nullptr,
                          stream_of(env));
@@ -814,4 +1145,79 @@ extern "C" int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const
   if ((rc = msb::cuda_check(cudaMemcpyAsync(v_out_h, a, n * sizeof(double), cudaMemcpyDeviceToHost, st), "D2H")))
     return rc;
   return msb::impl_sync(*S, st);
+}
+
+// ------------------------------------------------ decomposed sweep by steps
+static SweeperImpl* kba_impl(const Sweeper* sweeper) {
+  SweeperImpl* S = impl_of(sweeper);
+  if (!S) {
+    msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+    return nullptr;
+  }
+  if (!S->kba) {
+    msb::set_error(MSB_ERR_ARG, "the Sweeper is not decomposed (nproc_x * nproc_y == 1)");
+    return nullptr;
+  }
+  return S;
+}
+
+extern "C" int msb_kba_info(const Sweeper* sweeper, int* nstep, size_t* bytes_x, size_t* bytes_y) {
+  const SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  if (nstep) *nstep = S->kba->plan.nstep;
+  if (bytes_x) *bytes_x = S->kba->msg_bytes(0);
+  if (bytes_y) *bytes_y = S->kba->msg_bytes(1);
+  return MSB_OK;
+}
+
+extern "C" int msb_kba_set_buffers(Sweeper* sweeper, void* send_x, void* send_y, void* recv_x_lo, void* recv_x_hi,
+                                   void* recv_y_lo, void* recv_y_hi) {
+  SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  void* b[6] = {send_x, send_y, recv_x_lo, recv_x_hi, recv_y_lo, recv_y_hi};
+  for (int i = 0; i < 6; ++i) S->kba->buf[i] = b[i];
+  return MSB_OK;
+}
+
+extern "C" int msb_kba_begin(Sweeper* sweeper, double* vo_d, const double* vi_d, const Quantities* quan, Env* env) {
+  SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  if (!vo_d || !vi_d || !quan) return msb::set_error(MSB_ERR_ARG, "null argument");
+  int rc = msb::kba_own_buffers(*S);
+  if (rc) return rc;
+  const bool mats_on_dev = quan->a_from_m.d_ && quan->m_from_a.d_;
+  return msb::kba_begin(*S, vo_d, vi_d, quan->a_from_m.h_, quan->m_from_a.h_,
+                        mats_on_dev ? quan->a_from_m.d_ : nullptr, mats_on_dev ? quan->m_from_a.d_ : nullptr,
+                        stream_of(env));
+}
+
+extern "C" int msb_kba_step(Sweeper* sweeper, int step, Env* env) {
+  SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  if (step < 0 || step >= S->kba->plan.nstep) return msb::set_error(MSB_ERR_ARG, "step %d out of range", step);
+  return msb::kba_step(*S, step, stream_of(env));
+}
+
+extern "C" int msb_kba_messages(const Sweeper* sweeper, int step, msb_kba_msg* msgs, int max_msgs) {
+  const SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  if (step < 0 || step >= S->kba->plan.nstep) return msb::set_error(MSB_ERR_ARG, "step %d out of range", step);
+  std::vector<msb_kba_msg> v;
+  const int n = msb::kba_message_list(*S, step, v);
+  for (int i = 0; i < n && i < max_msgs; ++i) msgs[i] = v[i];
+  return n;
+}
+
+extern "C" int msb_kba_unpack(Sweeper* sweeper, int step, Env* env) {
+  SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  if (step < 0 || step >= S->kba->plan.nstep) return msb::set_error(MSB_ERR_ARG, "step %d out of range", step);
+  return msb::kba_unpack(*S, step, stream_of(env));
+}
+
+extern "C" int msb_kba_end(Sweeper* sweeper, Env* env) {
+  SweeperImpl* S = kba_impl(sweeper);
+  if (!S) return MSB_ERR_ARG;
+  int rc = msb::cuda_check(cudaStreamSynchronize(stream_of(env)), "sweep");
+  return S->kba->rc ? S->kba->rc : rc;
 }
