@@ -139,6 +139,9 @@ typedef void* Stream_t; /* a cudaStream_t */
 typedef double Timer;
 
 typedef struct msb_comm msb_comm;
+/* Env.flags_: several processes of the group drive the same GPU; their
+ * sweep kernels then take turns instead of sharing the GPU at once. */
+enum { MSB_ENV_SHARED_GPU = 1 };
 
 typedef struct {
   int nproc_x_;
@@ -150,7 +153,7 @@ typedef struct {
   int device_;
   int proc_;         /* this process's number in its group (0 without one) */
   int nproc_world_;  /* processes in the group (1 without one)             */
-  int pad_;
+  int flags_;        /* MSB_ENV_SHARED_GPU: processes of the group share GPUs */
   const msb_comm* comm_;
 } Env;
 
@@ -494,10 +497,12 @@ typedef struct {
 
 struct msb_comm {
   void* ctx;
-  /* Every process calls this after each step with the messages of that step
-   * (possibly none) and returns 0 once its receives have landed in device
-   * memory.  The device work that filled the send buffers has finished. */
-  int (*exchange)(void* ctx, const msb_kba_msg* msgs, int nmsg);
+  /* Every active process calls this after each step with the messages of
+   * that step (possibly none) and returns 0 once its sends and receives have
+   * completed in device memory.  The device work that filled the send
+   * buffers, and the unpacking of the previous step's receives, has
+   * finished. */
+  int (*exchange)(void* ctx, int nactive, const msb_kba_msg* msgs, int nmsg);
   /* The collectives run over the active processes 0 .. nactive - 1 (the
    * reference's active communicator, env_mpi.c:128-135), called by each of
    * them.  sum_double: *value = the sum of their *value (Env_sum_d).
@@ -531,8 +536,9 @@ int msb_kba_plan_messages(int nproc_x, int nproc_y, int nblock_z, int proc, int 
  *     then receives x from the lower / higher neighbour, y lower / higher),
  *     each at least the axis's bytes; NULL = buffers the sweeper allocates.
  *   msb_kba_begin: starts vo_d = sweep(vi_d) on the Env's stream.
- *   msb_kba_step: launches this process's slab of `step` (if any) and copies
- *     its leaving faces into the send buffers.
+ *   msb_kba_step: launches this process's slab of `step` (if any), copies
+ *     its leaving faces into the send buffers and waits for the Env's stream
+ *     (so the previous step's unpacking has finished too).
  *   msb_kba_messages: the step's messages with their buffers.
  *   msb_kba_unpack: after the receives of `step` landed: the entering faces
  *     into this process's face planes.

@@ -43,7 +43,7 @@ class Env(ctypes.Structure):
     _fields_ = [("nproc_x_", ctypes.c_int), ("nproc_y_", ctypes.c_int), ("tag_", ctypes.c_int),
                 ("is_proc_active_", ctypes.c_int), ("is_using_device_", ctypes.c_int),
                 ("stream_kernel_faces_", ctypes.c_void_p), ("device_", ctypes.c_int), ("proc_", ctypes.c_int),
-                ("nproc_world_", ctypes.c_int), ("pad_", ctypes.c_int), ("comm_", ctypes.c_void_p)]
+                ("nproc_world_", ctypes.c_int), ("flags_", ctypes.c_int), ("comm_", ctypes.c_void_p)]
 
 
 class KbaMsg(ctypes.Structure):
@@ -52,7 +52,7 @@ class KbaMsg(ctypes.Structure):
                 ("bytes", ctypes.c_size_t), ("buf", ctypes.c_void_p)]
 
 
-EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(KbaMsg), ctypes.c_int)
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(KbaMsg), ctypes.c_int)
 SUM_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
 ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_int))
@@ -240,8 +240,8 @@ def local_extent(n_global: int, nproc: int, proc: int):
 
 
 def make_comm(exchange, sum_double, allgather_int, barrier) -> Comm:
-    """msb_comm from Python callables: exchange(msgs) with msgs a list of
-    KbaMsg; sum_double(nactive, x) -> float; allgather_int(nactive, v) ->
+    """msb_comm from Python callables: exchange(nactive, msgs) with msgs a
+    list of KbaMsg; sum_double(nactive, x) -> float; allgather_int(nactive, v) ->
     list of ints; barrier(nactive) -- the collectives over the active
     processes 0 .. nactive - 1.  A callable that raises makes the call return
     -1.  Keep the result alive as long as an Env uses it (it holds the
@@ -257,8 +257,8 @@ def make_comm(exchange, sum_double, allgather_int, barrier) -> Comm:
                 return -1
         return call
 
-    def ex(_ctx, msgs, n):
-        exchange([msgs[i] for i in range(n)])
+    def ex(_ctx, nactive, msgs, n):
+        exchange(nactive, [msgs[i] for i in range(n)])
         return 0
 
     def sm(_ctx, nactive, v):

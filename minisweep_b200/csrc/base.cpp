@@ -147,6 +147,9 @@ extern "C" void Env_initialize(Env* env, int argc, char** argv) {
   env->nproc_x_ = 1;
   env->nproc_y_ = 1;
   env->is_proc_active_ = Bool_true;
+  // env_mpi.c:75-95 joins MPI_COMM_WORLD here: a process started by the
+  // node launcher joins its group (and takes its GPU) the same way
+  msb::insist_status(msb::node_attach(env), "Env_initialize: process group");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
   env->device_ = dev;
@@ -200,6 +203,7 @@ static const msb_comm* grid_comm(const Env* env) {
 extern "C" void Env_finalize(Env* env) {
   if (env->stream_kernel_faces_) cudaStreamDestroy((cudaStream_t)env->stream_kernel_faces_);
   env->stream_kernel_faces_ = nullptr;
+  msb::node_detach(env);
 }
 
 extern "C" Bool_t Env_is_proc_master(Env* env) { return Env_is_proc_active(env) && Env_proc_this(env) == 0; }

@@ -114,4 +114,10 @@ int build_kba_plan(int npx, int npy, int nblock, KbaPlan& out);
 int kba_unit_at(const KbaPlan& plan, int proc, int step);  // unit swept at the step, or -1
 int kba_messages(const KbaPlan& plan, int proc, int step, std::vector<KbaMsg>& msgs);
 
+// The node-local process group (node_comm.cpp): joined by Env_initialize when
+// the launcher's MSB_NPROC / MSB_PROC / MSB_GROUP are set; left by
+// Env_finalize.
+int node_attach(Env* env);
+void node_detach(Env* env);
+
 }  // namespace msb

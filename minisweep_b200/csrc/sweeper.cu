@@ -765,13 +765,15 @@ static int kba_begin(SweeperImpl& S, double* vo_d, const double* vi_d, const dou
 }
 
 // This process's unit of `step` (every pass), then its leaving faces into the
-// send buffers; waits for the device.  After an error the later steps launch
-// nothing, so that the process still takes part in every exchange.
+// send buffers; returns with the stream drained (the previous step's
+// unpacking included), so the receive buffers are free again.  After an
+// error the later steps launch nothing, so that the process still takes part
+// in every exchange.
 static int kba_step(SweeperImpl& S, int step, cudaStream_t stream) {
   KbaState& K = *S.kba;
   if (K.rc) return K.rc;
   const int k = kba_unit_at(K.plan, K.proc, step);
-  if (k < 0) return MSB_OK;
+  if (k < 0) return K.rc = cuda_check(cudaStreamSynchronize(stream), "sweep");
   const int oct = K.plan.unit_oct[k];
   int rc = MSB_OK;
   for (int c = 0; c < K.npass && !rc; ++c) {
@@ -877,21 +879,36 @@ static int kba_own_buffers(SweeperImpl& S) {
 }
 
 // A whole decomposed sweep with the transport of the Env's process group.
+// When processes of the group share a GPU, their slabs of a step run one
+// process after the other (a barrier between turns): no two processes' sweep
+// kernels are on one GPU at once.
 static int kba_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const double* afm_h, const double* mfa_h,
-                     const double* afm_d, const double* mfa_d, const msb_comm* comm, cudaStream_t stream) {
+                     const double* afm_d, const double* mfa_d, const Env* env, cudaStream_t stream) {
   KbaState& K = *S.kba;
+  const msb_comm* comm = env ? env->comm_ : nullptr;
   if (!comm) return set_error(MSB_ERR_ARG, "a decomposed sweep needs the Env's process group (msb_env_set_comm)");
+  const int nactive = K.plan.npx * K.plan.npy;
+  const bool turns = (env->flags_ & MSB_ENV_SHARED_GPU) != 0;
   int rc = kba_own_buffers(S);
   if (!rc) rc = kba_begin(S, vo_d, vi_d, afm_h, mfa_h, afm_d, mfa_d, stream);
   if (rc) K.rc = rc;
   std::vector<msb_kba_msg> msgs;
-  // every process takes every step's exchange, errors or not
+  // every process takes every step's barriers and exchange, errors or not
   for (int step = 0; step < K.plan.nstep; ++step) {
-    kba_step(S, step, stream);
+    if (turns) {
+      for (int q = 0; q < nactive; ++q) {
+        if (q == K.proc) kba_step(S, step, stream);
+        if (comm->barrier(comm->ctx, nactive) != 0 && !K.rc)
+          K.rc = set_error(MSB_ERR_ARG, "process group barrier failed at step %d", step);
+      }
+    } else {
+      kba_step(S, step, stream);
+    }
     const int n = kba_message_list(S, step, msgs);
-    if (comm->exchange(comm->ctx, msgs.data(), n) != 0 && !K.rc)
+    if (comm->exchange(comm->ctx, nactive, msgs.data(), n) != 0 && !K.rc)
       K.rc = set_error(MSB_ERR_ARG, "face exchange failed at step %d", step);
     kba_unpack(S, step, stream);
+    if (turns && !K.rc) K.rc = cuda_check(cudaStreamSynchronize(stream), "unpack faces");
   }
   if (!K.rc) K.rc = cuda_check(cudaStreamSynchronize(stream), "sweep");
   return K.rc;
@@ -1030,7 +1047,7 @@ extern "C" int Sweeper_sweep_device(Sweeper* sweeper, double* vo_d, const double
   if (S->kba)
     return msb::kba_sweep(*S, vo_d, vi_d, quan->a_from_m.h_, quan->m_from_a.h_,
                           mats_on_dev ? quan->a_from_m.d_ : nullptr, mats_on_dev ? quan->m_from_a.d_ : nullptr,
-                          env ? env->comm_ : nullptr, stream_of(env));
+                          env, stream_of(env));
   return msb::impl_sweep(*S, vo_d, vi_d, quan->a_from_m.h_, quan->m_from_a.h_,
                          mats_on_dev ? quan->a_from_m.d_ : nullptr, mats_on_dev ? quan->m_from_a.d_ : nullptr,
                          stream_of(env));

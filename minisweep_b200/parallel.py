@@ -104,9 +104,10 @@ class TorchGroupComm:
         problem.kba_set_buffers(*[b.data_ptr() for b in bufs])
         self.buffers = {b.data_ptr(): b for b in bufs}
 
-    def _exchange(self, msgs):
+    def _exchange(self, nactive, msgs):
         """All of one step's messages; returns after they landed."""
         torch, dist = self.torch, self.dist
+        self._whole(nactive)
         if not msgs:
             return
         views = [(m, self.buffers[m.buf][:m.bytes]) for m in msgs]

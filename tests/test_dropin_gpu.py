@@ -76,3 +76,48 @@ def test_reference_tester_battery(name, pairs):
     m = re.search(r"TESTS\s+(\d+)\s+PASSED\s+(\d+)\s+FAILED\s+(\d+)", out.stdout)
     assert m, out.stdout[-2000:]
     assert (int(m.group(1)), int(m.group(2)), int(m.group(3))) == (pairs, pairs, 0), out.stdout[-2000:]
+
+
+# --------------------------------------------- the MPI builds, as a process group
+# The reference's MPI configurations (tester.c:395-454 test_mpi with 16
+# processes; tester.c:290-391 test_cuda + :458-509 test_mpi_cuda with 4),
+# started by the node launcher in place of mpirun: the library's Env joins the
+# launcher's group, the decomposed sweeps exchange their faces between the
+# processes (CUDA IPC device copies), and the processes sharing this one GPU
+# take turns with their sweep kernels.
+def _launch(n, argv, timeout):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=root)
+    return subprocess.run([sys.executable, "-m", "minisweep_b200.launch", "-n", str(n), "--timeout",
+                           str(timeout), "--"] + argv, capture_output=True, text=True, timeout=timeout + 120,
+                          env=env)
+
+
+@pytest.mark.parametrize("name,nproc,pairs", [
+    ("tester_b200_mpi_nm16", 16, 6),
+    ("tester_b200_mpi_cuda_nm16", 4, 984 + 16),
+])
+def test_reference_mpi_tester_battery(name, nproc, pairs):
+    out = _launch(nproc, [binary(name)], 1500)
+    assert out.returncode == 0, out.stderr[-3000:]
+    m = re.search(r"TESTS\s+(\d+)\s+PASSED\s+(\d+)\s+FAILED\s+(\d+)", out.stdout)
+    assert m, out.stdout[-2000:]
+    assert (int(m.group(1)), int(m.group(2)), int(m.group(3))) == (pairs, pairs, 0), out.stdout[-3000:]
+
+
+@pytest.mark.parametrize("nproc,grid", [(2, "--nproc_x 2 --nproc_y 1"), (4, "--nproc_x 2 --nproc_y 2"),
+                                        (6, "--nproc_x 3 --nproc_y 2")])
+def test_reference_sweep_driver_decomposed(nproc, grid):
+    """sweep.c on a process grid prints the single-process normsq."""
+    flags = "--ncell_x 12 --ncell_y 9 --ncell_z 8 --ne 6 --na 32 --nblock_z 4 --niterations 2"
+    out = _launch(nproc, [binary("sweep_b200_nm16")] + (flags + " " + grid).split(), 600)
+    assert out.returncode == 0, out.stderr[-3000:]
+    m = re.search(r"Normsq result: ([0-9.e+]+)\s+diff: ([0-9.e+-]+)\s+(PASS|FAIL)", out.stdout)
+    assert m, out.stdout
+    assert m.group(3) == "PASS" and float(m.group(2)) == 0.0
+    single = subprocess.run([binary("sweep_b200_nm16")] + flags.split(), capture_output=True, text=True,
+                            timeout=300)
+    m1 = re.search(r"Normsq result: ([0-9.e+]+)", single.stdout)
+    assert m1 and m1.group(1) == m.group(1)

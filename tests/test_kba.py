@@ -96,7 +96,7 @@ def _fake_comm(gx, gy, npx, npy):
         n, np_ = (gx, npx) if axis == 0 else (gy, npy)
         return [msb.local_extent(n, np_, (q % npx) if axis == 0 else (q // npx))[1] for q in range(nactive)]
 
-    return msb.make_comm(lambda msgs: None, lambda nactive, x: x, allgather, lambda nactive: None)
+    return msb.make_comm(lambda nactive, msgs: None, lambda nactive, x: x, allgather, lambda nactive: None)
 
 
 @pytest.mark.parametrize("npx,npy", [(2, 1), (1, 3), (4, 4), (3, 2)])
@@ -218,7 +218,7 @@ def _group_rank(rank, world, port, npx, npy, out):
     if px > 0:
         msgs.append(msb.KbaMsg(rank - 1, 0, 0, 0, 64, recv.data_ptr()))
     arr = (msb.KbaMsg * max(1, len(msgs)))(*msgs)
-    rc = tg.comm.exchange(None, arr, len(msgs))  # the C entry point the library calls
+    rc = tg.comm.exchange(None, world, arr, len(msgs))  # the C entry point the library calls
     out[rank] = (q.ix_base, q.iy_base, q.ncell_x_g, q.ncell_y_g, s.value, d.value, rc, int(recv[0]), int(recv[-1]))
     L.Quantities_destroy(ctypes.byref(q))
     dist.barrier()
@@ -256,3 +256,47 @@ def test_group_transport_gloo(npx, npy):
         assert rc == 0
         if r % npx > 0:
             assert r0 == r1 == r - 1
+
+
+# ------------------------------------------------ the node-local group
+@pytest.mark.timeout(300)
+def test_node_group_collectives(tmp_path):
+    """Four processes started by the launcher join one group in
+    Env_initialize; grids of 1, 2, 3 and 4 of them run the library's
+    allgather (subdomain offsets) and sum (norms) through shared memory,
+    with the processes a grid leaves out going straight on to the next grid
+    (per-size barriers keep them apart, as the reference's per-run
+    communicators do)."""
+    import json
+    import os
+
+    from minisweep_b200 import launch
+
+    child = os.path.join(os.path.dirname(__file__), "kba_group_child.py")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="", PYTHONPATH=root)
+    assert launch.run(4, [sys.executable, child, str(tmp_path)], timeout=240, env=env) == 0
+    import kba_group_child as kc
+
+    # single-process reference: the whole initial state's sum of squares
+    L = msb.lib()
+    e1 = msb.Env()
+    L.Env_initialize(ctypes.byref(e1), 0, None)
+    q = msb.Quantities()
+    dims = msb.Dimensions(kc.GX, kc.GY, kc.NZ, kc.NE, kc.NM, kc.NA)
+    L.Quantities_create(ctypes.byref(q), dims, ctypes.byref(e1))
+    v = np.zeros(kc.GX * kc.GY * kc.NZ * kc.NE * kc.NM * 4)
+    L.initialize_state(v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), dims, 4, ctypes.byref(q))
+    L.Quantities_destroy(ctypes.byref(q))
+    d_ref = float(np.sum(v * v))
+    for p in range(4):
+        res = json.load(open(tmp_path / f"proc_{p}.json"))
+        assert (res["proc"], res["nproc"]) == (p, 4)
+        for (npx, npy), run in zip(kc.GRIDS, res["runs"]):
+            if p >= npx * npy:
+                assert run is None
+                continue
+            ixb, iyb, gx, gy, d = run
+            assert (ixb, iyb) == (msb.local_extent(kc.GX, npx, p % npx)[0], msb.local_extent(kc.GY, npy, p // npx)[0])
+            assert (gx, gy) == (kc.GX, kc.GY)
+            assert d == d_ref

@@ -36,7 +36,7 @@ def _group_comm(gx, gy, npx, npy):
         n, np_ = (gx, npx) if axis == 0 else (gy, npy)
         return [msb.local_extent(n, np_, (q % npx) if axis == 0 else (q // npx))[1] for q in range(nactive)]
 
-    return msb.make_comm(lambda msgs: None, lambda nactive, x: x, allgather, lambda nactive: None)
+    return msb.make_comm(lambda nactive, msgs: None, lambda nactive, x: x, allgather, lambda nactive: None)
 
 
 def sweep_decomposed(common, npx, npy, nblock_z, nm, vi_global, nsweep=1, extra=""):
