@@ -342,8 +342,8 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
 
 def measure_dense(args, dev, world: int, local_rank: int) -> dict | None:
     """The angle/group-heavy case: 32x32x96 cells, ne 128, na 128, NM 16,
-    nblock_z 12, built-in Quantities.  One FP64 sweep (two 64-angle passes,
-    tile shape autotuned by the untimed first sweep) against one sweep of each
+    nblock_z 12, built-in Quantities.  One FP64 sweep (kernel, tile shape,
+    task window and angle passes autotuned by the untimed first sweep) against one sweep of each
     mixed precision (four 32-angle passes), each timed after one untimed
     sweep; under torchrun each rank sweeps its own 128-group slice.  The FP64
     sweep of the built-in problem returns its input exactly, so the mixed
@@ -390,6 +390,7 @@ def measure_dense(args, dev, world: int, local_rank: int) -> dict | None:
                 r["exact"] = bool(torch.equal(va, vb))
                 r["tflops"] = flops / (ms * 1e-3) / 1e12
                 r["tile"] = pb.tile()
+                r["launches_per_sweep"] = (na + r["tile"]["angle_pass"] - 1) // r["tile"]["angle_pass"]
             else:
                 r["max_rel"] = (torch.max(torch.abs(vb - va)) / torch.max(torch.abs(va))).item()
                 nf = torch.sum(va * va)
@@ -701,7 +702,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
                                                          "best_other_tile": tile["ms_other"]}},
                     "plan": {"fp64_kernel": "chained wavefront" if tile["fp64_kernel"] else "staged",
                              "task_window_x_sms": tile["task_window"], "l2_hints": tile["l2_hints"],
-                             "plans_timed": tile["candidates"]},
+                             "angles_per_pass": tile["angle_pass"], "plans_timed": tile["candidates"]},
                     "roofline": roofline, "cpu_baseline": cpu,
                     "e2e": e2e,
                     "clocks": clk, "gpu_launches": args.steps * NITER,

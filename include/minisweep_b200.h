@@ -354,12 +354,15 @@ int Sweeper_last_stats(const Sweeper* sweeper, long long* ntask, int* nlaunch);
  * its CPU/GPU thread blocks. */
 int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_chosen, float* ms_other);
 /* The rest of the FP64 plan in use: the kernel (0 staged, 1 chained
- * wavefront), the task window (x SMs) of its schedule, the L2 policy flag, and
- * how many plans --autotune 1 timed (1 without it).  With --autotune 1 the
- * first sweep runs every candidate -- both kernels x both tile shapes x task
- * windows 4, 8 and 16 -- and keeps the fastest.  No reference counterpart
- * (the reference's tuning flags, sweeper_kba_c.h:54-233, are set by hand). */
-int Sweeper_plan(const Sweeper* sweeper, int* fp64_kernel, int* task_window, int* l2_hints, int* ncandidates);
+ * wavefront), the task window (x SMs) of its schedule, the L2 policy flag,
+ * how many plans --autotune 1 timed (1 without it), and the angles per pass
+ * (--angle_pass; na above it is swept in passes).  With --autotune 1 the
+ * first sweep runs every candidate -- both kernels (the staged one with 64-
+ * and with 32-angle passes when na > 32) x both tile shapes x task windows 4,
+ * 8 and 16 -- and keeps the fastest.  No reference counterpart (the
+ * reference's tuning flags, sweeper_kba_c.h:54-233, are set by hand). */
+int Sweeper_plan(const Sweeper* sweeper, int* fp64_kernel, int* task_window, int* l2_hints, int* ncandidates,
+                 int* angle_pass);
 /* Copy of the schedule (one record of MSB_TASK_INTS ints per task, in launch
  * order) for host-side checks; returns the task count, or <0. */
 enum { MSB_TASK_INTS = 16 };

@@ -139,7 +139,7 @@ def lib() -> ctypes.CDLL:
         L.Sweeper_set_spin_limit.argtypes = [P(Sweeper), ctypes.c_longlong]
         L.Sweeper_tile.argtypes = [P(Sweeper), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_float),
                                    P(ctypes.c_float)]
-        L.Sweeper_plan.argtypes = [P(Sweeper), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+        L.Sweeper_plan.argtypes = [P(Sweeper)] + [P(ctypes.c_int)] * 5
         L.msb_state_norms_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, P(D), P(D), P(Env)]
         L.msb_initialize_state_device.argtypes = [ctypes.c_void_p, Dimensions, P(Env)]
         L.msb_initialize_state_slice_device.argtypes = [ctypes.c_void_p, Dimensions, ctypes.c_int, P(Env)]
@@ -429,10 +429,11 @@ class Problem:
         _check(lib().Sweeper_tile(ctypes.byref(self.sweeper), ctypes.byref(tx), ctypes.byref(ty), ctypes.byref(a),
                                   ctypes.byref(b)))
         out = {"tx": tx.value, "ty": ty.value, "ms_chosen": a.value, "ms_other": b.value}
-        k, w, h, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        k, w, h, n, ap = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(lib().Sweeper_plan(ctypes.byref(self.sweeper), ctypes.byref(k), ctypes.byref(w), ctypes.byref(h),
-                                  ctypes.byref(n)))
-        out.update(fp64_kernel=k.value, task_window=w.value, l2_hints=h.value, candidates=n.value)
+                                  ctypes.byref(n), ctypes.byref(ap)))
+        out.update(fp64_kernel=k.value, task_window=w.value, l2_hints=h.value, candidates=n.value,
+                   angle_pass=ap.value)
         return out
 
     def set_timeout_ns(self, ns: int) -> None:

@@ -129,9 +129,10 @@ Variant pick_chain(int tile) {
 // precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves.
 // tile: 0 = the default shape, 42 or 24 (FP64 only).  kernel (FP64 only):
 // 0 = the staged kernel, up to 64 angles per pass; 1 = the chained-wavefront
-// kernel, 32 angles per pass.  na <= 128; the mixed kernels sweep 32 angles
-// per pass.
-Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0) {
+// kernel, 32 angles per pass.  angle_pass (staged kernel): 0 = 64 angles per
+// pass when na > 32, else 32; 32 or 64 = that many.  na <= 128; the mixed
+// kernels sweep 32 angles per pass.
+Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0, int angle_pass = 0) {
   if (na > 128) return Variant();
   if (precision == 1 || precision == 2) {
     if (tile != 0) return Variant();
@@ -146,7 +147,7 @@ Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0
       default: return Variant();
     }
   }
-  const int nch = na > 32 ? 2 : 1;
+  const int nch = angle_pass == 32 ? 1 : angle_pass == 64 ? 2 : na > 32 ? 2 : 1;
   switch (nm) {
     case 4: return pick_nch<4>(nch, tile);
     case 8: return pick_nch<8>(nch, tile);
@@ -325,12 +326,12 @@ static int setup_plan(const SweeperImpl& S, const Variant& var, int window, Sche
 }
 
 static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, int tile = 0, bool autotune = false,
-                       int kernel = 0) {
+                       int kernel = 0, int angle_pass = 0) {
   S.dims = dims;
   S.precision = precision;
   if (dims.ncell_x <= 0 || dims.ncell_y <= 0 || dims.ncell_z <= 0 || dims.ne <= 0 || dims.na <= 0)
     return set_error(MSB_ERR_ARG, "invalid dimensions");
-  S.var = pick_variant(dims.nm, dims.na, precision, tile, kernel);
+  S.var = pick_variant(dims.nm, dims.na, precision, tile, kernel, angle_pass);
   if (!S.var.valid())
     return set_error(MSB_ERR_UNSUPPORTED,
                      "no kernel variant for nm=%d na=%d precision=%d tile=%d (nm in {4,8,16}; na <= 128; "
@@ -346,18 +347,22 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
   if ((rc = setup_plan(S, S.var, S.window, S.sched, S.gp_block, S.d_tasks, S.grid))) return rc;
   long long ntask = S.sched.ntask();
   if (autotune) {
-    // candidates: both FP64 kernels x both tile shapes x task windows of 4,
-    // 8 and 16 x SMs, besides the sweeper's own plan
+    // candidates: both FP64 kernels (the staged one with 64- and 32-angle
+    // passes when na > 32) x both tile shapes x task windows of 4, 8 and 16
+    // x SMs, besides the sweeper's own plan
     S.autotune = true;
     const int windows[3] = {4, 8, 16};
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 3; ++k)
       for (int t = 0; t < 2; ++t)
         for (int w : windows) {
-          const int tile_c = t == 0 ? 42 : 24;
-          const bool is_main = k == kernel && (S.var.tx == 4) == (t == 0) && w == S.window;
+          if (k == 2 && dims.na <= 32) continue;  // the staged kernel's passes differ only above 32 angles
+          const int tile_c = t == 0 ? 42 : 24, kern = k == 2 ? 0 : k, pass_c = k == 2 ? 32 : 0;
+          Variant v = pick_variant(dims.nm, dims.na, precision, tile_c, kern, pass_c);
+          const bool is_main =
+              v.kernel == S.var.kernel && v.pass == S.var.pass && v.tx == S.var.tx && w == S.window;
           if (is_main) continue;
           AltPlan a;
-          a.var = pick_variant(dims.nm, dims.na, precision, tile_c, k);
+          a.var = v;
           a.window = w;
           a.l2_hints = S.l2_hints;
           if ((rc = setup_plan(S, a.var, a.window, a.sched, a.gp_block, a.d_tasks, a.grid))) {
@@ -990,6 +995,12 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // FP64 sweep kernel: 0 = the staged kernel (default), 1 = the chained wavefront
   const int fp64_kernel = Arguments_consume_int_or_default(args, "--fp64_kernel", 0);
   if (fp64_kernel != 0 && fp64_kernel != 1) return msb::set_error(MSB_ERR_ARG, "--fp64_kernel must be 0 or 1");
+  // angles per pass of the staged FP64 kernel: 0 = 64 above 32 angles, else 32
+  const int angle_pass = Arguments_consume_int_or_default(args, "--angle_pass", 0);
+  if (angle_pass != 0 && angle_pass != 32 && angle_pass != 64)
+    return msb::set_error(MSB_ERR_ARG, "--angle_pass must be 0, 32 or 64");
+  if (angle_pass != 0 && (fp64_kernel != 0 || sweeper->precision != 0))
+    return msb::set_error(MSB_ERR_ARG, "--angle_pass applies to the staged FP64 kernel (--fp64_kernel 0, --precision 0)");
   // tasks between a tile and its downwind neighbour in the schedule, in
   // multiples of the SM count
   const int task_window = Arguments_consume_int_or_default(args, "--task_window", 4);
@@ -1021,7 +1032,7 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
     rc = msb::impl_create_kba(*S, dims, tile, sweeper->nblock_z, Env_nproc_x(env), Env_nproc_y(env),
                               Env_proc_this(env), quan->ix_base + 3 * quan->iy_base);
   } else {
-    rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0, fp64_kernel);
+    rc = msb::impl_create(*S, dims, sweeper->precision, tile, autotune != 0, fp64_kernel, angle_pass);
   }
   if (rc) return rc;
   sweeper->impl_ = S.release();
@@ -1107,13 +1118,14 @@ extern "C" int Sweeper_tile(const Sweeper* sweeper, int* tx, int* ty, float* ms_
 }
 
 extern "C" int Sweeper_plan(const Sweeper* sweeper, int* fp64_kernel, int* task_window, int* l2_hints,
-                            int* ncandidates) {
+                            int* ncandidates, int* angle_pass) {
   const SweeperImpl* S = impl_of(sweeper);
   if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
   if (fp64_kernel) *fp64_kernel = S->var.kernel;
   if (task_window) *task_window = S->window;
   if (l2_hints) *l2_hints = S->l2_hints;
   if (ncandidates) *ncandidates = S->autotune ? 1 + (int)S->alts.size() : 1;
+  if (angle_pass) *angle_pass = S->var.pass;
   return MSB_OK;
 }
 

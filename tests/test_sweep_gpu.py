@@ -89,6 +89,9 @@ def test_builtin_flags_invariant(extra):
     (4, 5, 3, 2, 100, 4, "--autotune 1"),    # a ragged last angle pass
     (7, 6, 5, 4, 64, 16, "--tile 24 --fp64_kernel 1"),
     (4, 5, 3, 2, 100, 4, "--autotune 1 --fp64_kernel 1"),
+    (5, 4, 3, 3, 128, 16, "--angle_pass 32"),   # four 32-angle passes of the staged kernel
+    (6, 5, 4, 3, 40, 8, "--angle_pass 32 --tile 24"),
+    (4, 5, 3, 2, 20, 4, "--angle_pass 64"),     # a 64-angle pass over 20 angles
 ])
 def test_tile_shapes_bitexact(nx, ny, nz, ne, na, nm, extra):
     # the 2 x 4 tile (and the autotuned choice, whose first sweep runs both
@@ -106,6 +109,8 @@ def test_tile_shapes_bitexact(nx, ny, nz, ne, na, nm, extra):
         assert 0.0 < t["ms_chosen"] <= t["ms_other"]
     elif "--tile 24" in extra:
         assert (t["tx"], t["ty"]) == (2, 4)
+    if "--angle_pass" in extra:
+        assert t["angle_pass"] == int(extra.split("--angle_pass ")[1].split()[0])
 
 
 RANDOM = [
