@@ -128,10 +128,11 @@ Variant pick_chain(int tile) {
 
 // precision 0: FP64; 1: mixed with FP16 halves; 2: mixed with BF16 halves.
 // tile: 0 = the default shape, 42 or 24 (FP64 only).  kernel (FP64 only):
-// 0 = the staged kernel, up to 64 angles per pass; 1 = the chained-wavefront
-// kernel, 32 angles per pass.  angle_pass (staged kernel): 0 = 64 angles per
-// pass when na > 32, else 32; 32 or 64 = that many.  na <= 128; the mixed
-// kernels sweep 32 angles per pass.
+// 0 = the staged kernel, 32 or 64 angles per pass; 1 = the chained-wavefront
+// kernel, 32 angles per pass.  angle_pass (staged kernel): 0 or 32 = 32
+// angles per pass (the transform matrices stay in registers), 64 = two
+// 32-angle chunks per pass (matrices read from shared memory; slower per
+// angle).  na <= 128; the mixed kernels sweep 32 angles per pass.
 Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0, int angle_pass = 0) {
   if (na > 128) return Variant();
   if (precision == 1 || precision == 2) {
@@ -147,7 +148,7 @@ Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0
       default: return Variant();
     }
   }
-  const int nch = angle_pass == 32 ? 1 : angle_pass == 64 ? 2 : na > 32 ? 2 : 1;
+  const int nch = angle_pass == 64 ? 2 : 1;
   switch (nm) {
     case 4: return pick_nch<4>(nch, tile);
     case 8: return pick_nch<8>(nch, tile);
@@ -347,7 +348,7 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
   if ((rc = setup_plan(S, S.var, S.window, S.sched, S.gp_block, S.d_tasks, S.grid))) return rc;
   long long ntask = S.sched.ntask();
   if (autotune) {
-    // candidates: both FP64 kernels (the staged one with 64- and 32-angle
+    // candidates: both FP64 kernels (the staged one with 32- and 64-angle
     // passes when na > 32) x both tile shapes x task windows of 4, 8 and 16
     // x SMs, besides the sweeper's own plan
     S.autotune = true;
@@ -356,7 +357,7 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
       for (int t = 0; t < 2; ++t)
         for (int w : windows) {
           if (k == 2 && dims.na <= 32) continue;  // the staged kernel's passes differ only above 32 angles
-          const int tile_c = t == 0 ? 42 : 24, kern = k == 2 ? 0 : k, pass_c = k == 2 ? 32 : 0;
+          const int tile_c = t == 0 ? 42 : 24, kern = k == 2 ? 0 : k, pass_c = k == 2 ? 64 : 0;
           Variant v = pick_variant(dims.nm, dims.na, precision, tile_c, kern, pass_c);
           const bool is_main =
               v.kernel == S.var.kernel && v.pass == S.var.pass && v.tx == S.var.tx && w == S.window;
@@ -995,7 +996,7 @@ extern "C" int Sweeper_create_status(Sweeper* sweeper, Dimensions dims, const Qu
   // FP64 sweep kernel: 0 = the staged kernel (default), 1 = the chained wavefront
   const int fp64_kernel = Arguments_consume_int_or_default(args, "--fp64_kernel", 0);
   if (fp64_kernel != 0 && fp64_kernel != 1) return msb::set_error(MSB_ERR_ARG, "--fp64_kernel must be 0 or 1");
-  // angles per pass of the staged FP64 kernel: 0 = 64 above 32 angles, else 32
+  // angles per pass of the staged FP64 kernel: 0 or 32 = 32, 64 = two chunks per pass
   const int angle_pass = Arguments_consume_int_or_default(args, "--angle_pass", 0);
   if (angle_pass != 0 && angle_pass != 32 && angle_pass != 64)
     return msb::set_error(MSB_ERR_ARG, "--angle_pass must be 0, 32 or 64");

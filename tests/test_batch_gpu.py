@@ -32,8 +32,9 @@ def flags(p):
 
 def single(p, vi, a=None, m=None, niter=1):
     # the problem's own Sweeper with the kernel the batch uses (the staged
-    # FP64 kernel, 64-angle passes): same summation order, same bits
-    with msb.Problem(flags(p) + " --fp64_kernel 0", nm=p["nm"]) as pb:
+    # FP64 kernel, one pass of up to 64 angles): same summation order, same bits
+    with msb.Problem(flags(p) + " --fp64_kernel 0" + (" --angle_pass 64" if p["na"] > 32 else ""),
+                     nm=p["nm"]) as pb:
         if a is not None:
             pb.set_matrices(a, m)
         v = vi
