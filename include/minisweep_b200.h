@@ -411,14 +411,14 @@ int msb_sweep_noalloc(double* vo_d, const double* vi_d, const double* a_from_m_d
  * built-in or the caller's transform matrices), with results identical bit
  * for bit.
  *
- * Each problem has its own sizes (nm 4, 8 or 16; na <= 64) and its own device
+ * Each problem has its own sizes (nm 4, 8 or 16; na <= 128) and its own device
  * arrays in the reference layouts: vi/vo the state (16-byte aligned),
  * a_from_m [octant][im][ia] and m_from_a [octant][ia][im].  The face planes
  * are scratch from one device arena of scratch_bytes (0: what all problems
  * need at once, capped at 80 % of the free device memory); problems that do
  * not fit at once reuse the bytes of problems that completed earlier in the
  * same launch.  autotune != 0 times the two tile shapes (4 x 2 and 2 x 4
- * cells) on the median problem of each (nm, angle chunk) group at creation;
+ * cells) on the median problem of each nm group at creation;
  * those trial sweeps write that problem's vo.  Asynchronous calls run on the
  * given stream (a cudaStream_t, NULL = the legacy default stream); their
  * device status is checked by msb_batch_sync. */
@@ -461,15 +461,20 @@ int msb_batch_sync(msb_batch* b, void* stream);
 int msb_batch_problem_ms(const msb_batch* b, double* ms, int n);
 int msb_batch_info(const msb_batch* b, msb_batch_info_t* info);
 /* Host-only planning of the same batch for nsm SMs (no device, pointers may
- * be NULL) for host-side checks; bit (3 * (nch - 1) + k) of tile24_mask, k = 0,
- * 1, 2 for nm 4, 8, 16, selects the 2 x 4 tile for that group. */
+ * be NULL) for host-side checks; bit k of tile24_mask, k = 0, 1, 2 for nm 4,
+ * 8, 16, selects the 2 x 4 tile for that group. */
 int msb_batch_plan(msb_batch** out, const msb_problem* problems, int nproblem, int nsm,
                    size_t scratch_bytes, int tile24_mask);
+/* A batch sweeps every problem in entries of 32 angles, as a Sweeper sweeps
+ * them in passes: entry e is problem problem[e]'s angles [angle0[e],
+ * angle0[e] + 32); later entries of a problem add to vo after the entry
+ * before them completed.  Returns the entry count. */
+int msb_batch_entries(const msb_batch* b, int* problem, int* angle0, int max_entries);
 /* The planned task table (global ids, MSB_TASK_INTS ints per task) and the
- * problem of each task; returns the task count. */
+ * entry of each task; returns the task count. */
 long long msb_batch_tasks(const msb_batch* b, int* rec, int* prob, long long max_tasks);
-/* Arena placement per problem (offset, bytes) and the problems each one waits
- * for (pred[pred_off[p] .. pred_off[p + 1])); returns the predecessor count. */
+/* Arena placement per entry (offset, bytes) and the entries each one waits
+ * for (pred[pred_off[e] .. pred_off[e + 1])); returns the predecessor count. */
 int msb_batch_scratch(const msb_batch* b, long long* offset, long long* bytes, int* pred_off, int* pred,
                       int max_pred);
 /* Test hook: time budget (ns) of every device wait; 0 = default (4 s). */

@@ -158,6 +158,7 @@ def lib() -> ctypes.CDLL:
         L.msb_batch_info.argtypes = [ctypes.c_void_p, P(BatchInfo)]
         L.msb_batch_tasks.argtypes = [ctypes.c_void_p, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_longlong]
         L.msb_batch_tasks.restype = ctypes.c_longlong
+        L.msb_batch_entries.argtypes = [ctypes.c_void_p, P(ctypes.c_int), P(ctypes.c_int), ctypes.c_int]
         L.msb_batch_scratch.argtypes = [ctypes.c_void_p, P(ctypes.c_longlong), P(ctypes.c_longlong),
                                         P(ctypes.c_int), P(ctypes.c_int), ctypes.c_int]
         L.msb_batch_set_spin_limit.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
@@ -601,8 +602,21 @@ class Batch:
                     classes=[dict(nm=i.class_nm[c], nch=i.class_nch[c], tile=(i.class_tx[c], i.class_ty[c]),
                                   ntask=i.class_ntask[c]) for c in range(nc)])
 
+    def entries(self):
+        """(problem, first angle) of every entry: the batch sweeps each problem
+        in entries of 32 angles, as a Sweeper sweeps it in passes."""
+        L = lib()
+        n = L.msb_batch_entries(self._h, None, None, 0)
+        if n < 0:
+            raise SweepError(n, last_error())
+        prob = np.zeros(n, dtype=np.int32)
+        a0 = np.zeros(n, dtype=np.int32)
+        IP = ctypes.POINTER(ctypes.c_int)
+        L.msb_batch_entries(self._h, prob.ctypes.data_as(IP), a0.ctypes.data_as(IP), n)
+        return prob, a0
+
     def tasks(self):
-        """(table: ntask x 16 ints with global dependency ids, problem of each task)."""
+        """(table: ntask x 16 ints with global dependency ids, entry of each task)."""
         L = lib()
         n = L.msb_batch_tasks(self._h, None, None, 0)
         rec = np.zeros((n, TASK_INTS), dtype=np.int32)
@@ -612,11 +626,12 @@ class Batch:
         return rec, prob
 
     def scratch(self):
-        """(offset, bytes, pred_off, pred) of the face-scratch arena placement."""
+        """(offset, bytes, pred_off, pred) of the face-scratch arena placement, per entry."""
         L = lib()
-        off = np.zeros(self.n, dtype=np.int64)
-        nb = np.zeros(self.n, dtype=np.int64)
-        po = np.zeros(self.n + 1, dtype=np.int32)
+        ne = L.msb_batch_entries(self._h, None, None, 0)
+        off = np.zeros(ne, dtype=np.int64)
+        nb = np.zeros(ne, dtype=np.int64)
+        po = np.zeros(ne + 1, dtype=np.int32)
         LP, IP = ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int)
         npred = L.msb_batch_scratch(self._h, off.ctypes.data_as(LP), nb.ctypes.data_as(LP), po.ctypes.data_as(IP),
                                     None, 0)

@@ -52,8 +52,16 @@ constexpr size_t kAlign = 256;
 
 inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
+// One entry of the batch: one 32-angle pass of a caller's problem.  A
+// problem of na angles has ceil(na / 32) entries; entry c sweeps angles
+// [32 c, 32 c + nac) reading the caller's matrices in place, adds to vo from
+// the second pass on, uses the first pass's face scratch and starts once the
+// pass before it has completed (the order a Sweeper's passes run in, so the
+// sums are the same).
 struct ProbPlan {
   msb_problem d;
+  int user = 0, pass = 0, npass = 1, a0 = 0, nac = 0;
+  int prev = -1, next = -1;  // entries of the neighbouring passes
   int nch = 0, ngp = 0, kind = 0, cls = 0, tx = 4, ty = 2;
   Schedule sched;
   size_t face_bytes[3] = {0, 0, 0};
@@ -76,7 +84,8 @@ double step_cost(int nm, int nch) { return (0.3 + 0.7 * nm / 16.0) * nch; }
 }  // namespace
 
 struct BatchImpl {
-  std::vector<ProbPlan> probs;
+  std::vector<ProbPlan> probs;  // entries (angle passes of the caller's problems)
+  int nuser = 0;                // the caller's problems
   std::vector<ClassInfo> classes;
   int nsm = 0;
   bool device = false;
@@ -133,7 +142,7 @@ int check_problem(const msb_problem& p, int i, bool need_ptrs) {
     return set_error(MSB_ERR_ARG, "batch problem %d: invalid sizes", i);
   if (p.nm != 4 && p.nm != 8 && p.nm != 16)
     return set_error(MSB_ERR_UNSUPPORTED, "batch problem %d: nm %d (4, 8 or 16)", i, p.nm);
-  if (p.na > 64) return set_error(MSB_ERR_UNSUPPORTED, "batch problem %d: na %d (a batch takes na <= 64)", i, p.na);
+  if (p.na > 128) return set_error(MSB_ERR_UNSUPPORTED, "batch problem %d: na %d (a batch takes na <= 128)", i, p.na);
   if (need_ptrs) {
     if (!p.vi || !p.vo || !p.a_from_m || !p.m_from_a)
       return set_error(MSB_ERR_ARG, "batch problem %d: null device pointer", i);
@@ -146,7 +155,7 @@ int check_problem(const msb_problem& p, int i, bool need_ptrs) {
 // Per-problem schedule and sizes for the given tile of its class.
 int plan_problem(ProbPlan& P, int nsm) {
   const msb_problem& d = P.d;
-  P.nch = (d.na + 31) / 32;
+  P.nch = 1;
   P.ngp = (d.ne + 1) / 2;
   // the same task window as a single problem's schedule (4 x SMs)
   const int gpb = pick_gp_block(d.ncell_x, d.ncell_y, P.ngp, P.tx, P.ty, 4 * nsm);
@@ -311,16 +320,26 @@ int simulate_and_order(BatchImpl& B) {
   for (int p = 0; p < np; ++p) by_seq[B.probs[p].seq] = p;
   Arena arena(B.arena_bytes);
   int next_admit = 0;
+  auto push_ready = [&](int p) {
+    for (long long t = first[p]; t < first[p + 1]; ++t)
+      if (left[t] == 0) ready[B.probs[p].cls].push({B.probs[p].seq, t});
+  };
   auto admit = [&]() {
     while (next_admit < np) {
-      ProbPlan& P = B.probs[by_seq[next_admit]];
-      size_t off = 0;
-      if (!arena.alloc(P.scratch, &off)) break;
-      P.offset = off;
-      P.preds = arena.take(off, P.scratch, by_seq[next_admit]);
       const int p = by_seq[next_admit];
-      for (long long t = first[p]; t < first[p + 1]; ++t)
-        if (left[t] == 0) ready[P.cls].push({P.seq, t});
+      ProbPlan& P = B.probs[p];
+      if (P.prev >= 0) {
+        // a later pass: the first pass's scratch, after the pass before it
+        P.offset = B.probs[P.prev].offset;
+        P.preds = arena.take(P.offset, P.scratch, p);
+        if (pdone[P.prev] == B.probs[P.prev].sched.ntask()) push_ready(p);
+      } else {
+        size_t off = 0;
+        if (!arena.alloc(P.scratch, &off)) break;
+        P.offset = off;
+        P.preds = arena.take(off, P.scratch, p);
+        push_ready(p);
+      }
       ++next_admit;
     }
   };
@@ -362,8 +381,13 @@ int simulate_and_order(BatchImpl& B) {
       release(e.g, false);
       const int p = tprob[e.g];
       if (++pdone[p] == B.probs[p].sched.ntask()) {
-        arena.release(B.probs[p].offset, B.probs[p].scratch);
-        admit();
+        const ProbPlan& P = B.probs[p];
+        if (P.next >= 0) {
+          if (B.probs[P.next].seq < next_admit) push_ready(P.next);  // admitted, waiting for this pass
+        } else {
+          arena.release(P.offset, P.scratch);
+          admit();
+        }
       }
     }
   }
@@ -448,16 +472,33 @@ void make_classes(BatchImpl& B, const std::map<std::pair<int, int>, bool>& tile2
 // scratch capped at `cap`) and the task table.
 int plan_batch(BatchImpl& B, const msb_problem* probs, int n, const std::map<std::pair<int, int>, bool>& tile24,
                size_t scratch_bytes, size_t cap) {
-  B.probs.assign(n, ProbPlan());
+  // one entry per 32-angle pass of every problem
+  B.probs.clear();
+  B.nuser = n;
+  std::vector<int> first_entry(n);
   for (int i = 0; i < n; ++i) {
-    B.probs[i].d = probs[i];
-    B.probs[i].nch = (probs[i].na + 31) / 32;
-    auto it = tile24.find({probs[i].nm, B.probs[i].nch});
+    const int npass = (probs[i].na + 31) / 32;
+    first_entry[i] = (int)B.probs.size();
+    auto it = tile24.find({probs[i].nm, 1});
     const bool t24 = it != tile24.end() && it->second;
-    B.probs[i].tx = t24 ? 2 : 4;
-    B.probs[i].ty = t24 ? 4 : 2;
+    for (int c = 0; c < npass; ++c) {
+      ProbPlan e;
+      e.d = probs[i];
+      e.user = i;
+      e.pass = c;
+      e.npass = npass;
+      e.a0 = 32 * c;
+      e.nac = std::min(32, probs[i].na - 32 * c);
+      e.prev = c > 0 ? (int)B.probs.size() - 1 : -1;
+      e.nch = 1;
+      e.tx = t24 ? 2 : 4;
+      e.ty = t24 ? 4 : 2;
+      if (c > 0) B.probs.back().next = (int)B.probs.size();
+      B.probs.push_back(e);
+    }
   }
   // the problems' schedules are independent: build them on the host's cores
+  // (a problem's passes share its schedule)
   std::vector<int> prc(n, MSB_OK);
   {
     const int nthr = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
@@ -465,16 +506,26 @@ int plan_batch(BatchImpl& B, const msb_problem* probs, int n, const std::map<std
     std::vector<std::thread> pool;
     for (int t = 0; t < nthr; ++t)
       pool.emplace_back([&]() {
-        for (int i = next++; i < n; i = next++) prc[i] = plan_problem(B.probs[i], B.nsm);
+        for (int i = next++; i < n; i = next++) prc[i] = plan_problem(B.probs[first_entry[i]], B.nsm);
       });
     for (auto& th : pool) th.join();
   }
   for (int i = 0; i < n; ++i)
-    if (prc[i]) return plan_problem(B.probs[i], B.nsm);  // again on this thread: its error message
+    if (prc[i]) return plan_problem(B.probs[first_entry[i]], B.nsm);  // again on this thread: its error message
+  for (auto& e : B.probs)
+    if (e.pass > 0) {
+      const ProbPlan& f = B.probs[e.prev];
+      e.ngp = f.ngp;
+      e.sched = f.sched;
+      for (int k = 0; k < 3; ++k) e.face_bytes[k] = f.face_bytes[k];
+      e.scratch = f.scratch;
+      e.work = f.work;
+    }
   make_classes(B, tile24);
   if ((int)B.classes.size() > kMaxBatchClasses) return set_error(MSB_ERR_ARG, "batch: too many classes");
   size_t need = 0;
-  for (auto& p : B.probs) need += p.scratch;
+  for (auto& p : B.probs)
+    if (p.pass == 0) need += p.scratch;
   B.arena_bytes = scratch_bytes ? scratch_bytes : std::min(need, cap);
   return simulate_and_order(B);
 }
@@ -524,8 +575,10 @@ int upload_batch(BatchImpl& B) {
     Fp64Prob& q = pv[i];
     q.vi = P.d.vi;
     q.vo = P.d.vo;
-    q.afm = P.d.a_from_m;
-    q.mfa = P.d.m_from_a;
+    // the pass's angles of the caller's matrices, read in place
+    q.afm = P.d.a_from_m ? P.d.a_from_m + P.a0 : nullptr;
+    q.mfa = P.d.m_from_a ? P.d.m_from_a + (size_t)P.a0 * P.d.nm : nullptr;
+    q.a_stride = P.d.na;
     unsigned char* base = static_cast<unsigned char*>(B.d_arena) + P.offset;
     q.fxy = reinterpret_cast<double*>(base);
     q.fxz = reinterpret_cast<double*>(base + P.face_bytes[0]);
@@ -534,10 +587,10 @@ int upload_batch(BatchImpl& B) {
     q.ny = P.d.ncell_y;
     q.nz = P.d.ncell_z;
     q.ne = P.d.ne;
-    q.na = P.d.na;
+    q.na = P.nac;
     q.ngp = P.ngp;
-    q.ia_base = 0;
-    q.vo_add = 0;
+    q.ia_base = P.a0;
+    q.vo_add = P.pass > 0 ? 1 : 0;
     q.ie_base = 0;
   }
   if ((rc = upload(&B.d_tasks, B.rec, "batch tasks"))) return rc;
@@ -605,13 +658,13 @@ int sync_status(BatchImpl& B, cudaStream_t st) {
   return MSB_OK;
 }
 
-// Times both tile shapes on the median problem of each (nm, nch) group and
-// returns the faster shape per group.  The trial sweeps write that problem's
+// Times both tile shapes on the median problem of each nm group (every
+// entry sweeps one 32-angle chunk) and returns the faster shape per group.  The trial sweeps write that problem's
 // vo array (the batch's own sweeps overwrite it later).
 int autotune(const msb_problem* probs, int n, int nsm, size_t arena, std::map<std::pair<int, int>, bool>* tile24,
              double* tune_ms) {
   std::map<std::pair<int, int>, std::vector<int>> groups;
-  for (int i = 0; i < n; ++i) groups[{probs[i].nm, (probs[i].na + 31) / 32}].push_back(i);
+  for (int i = 0; i < n; ++i) groups[{probs[i].nm, 1}].push_back(i);
   cudaStream_t st = nullptr;
   int rc = cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "autotune stream");
   if (rc) return rc;
@@ -729,11 +782,10 @@ extern "C" int msb_batch_plan(msb_batch** out, const msb_problem* problems, int 
   if (!b) return msb::set_error(MSB_ERR_ARG, "out of host memory");
   BatchImpl& B = b->impl;
   B.nsm = nsm;
-  // bit (3 * (nch - 1) + nm index) of the mask selects the 2 x 4 tile
+  // bit (nm index) of the mask selects the 2 x 4 tile
   std::map<std::pair<int, int>, bool> tile24;
   const int nms[3] = {4, 8, 16};
-  for (int nch = 1; nch <= 2; ++nch)
-    for (int k = 0; k < 3; ++k) tile24[{nms[k], nch}] = ((tile24_mask >> (3 * (nch - 1) + k)) & 1) != 0;
+  for (int k = 0; k < 3; ++k) tile24[{nms[k], 1}] = ((tile24_mask >> k) & 1) != 0;
   if ((rc = msb::plan_batch(B, problems, nproblem, tile24, scratch_bytes, ~(size_t)0))) return rc;
   *out = b.release();
   return MSB_OK;
@@ -789,12 +841,14 @@ extern "C" int msb_batch_problem_ms(const msb_batch* b, double* ms, int n) {
   if (!b || !b->impl.device || !ms) return msb::set_error(MSB_ERR_ARG, "batch: invalid argument");
   const BatchImpl& B = b->impl;
   const int np = (int)B.probs.size();
-  if (n < np) return msb::set_error(MSB_ERR_ARG, "batch: output holds %d values, %d problems", n, np);
+  if (n < B.nuser) return msb::set_error(MSB_ERR_ARG, "batch: output holds %d values, %d problems", n, B.nuser);
   std::vector<long long> t(np + 1);
   int rc = msb::cuda_check(cudaMemcpy(t.data(), B.d_ptime, (np + 1) * sizeof(long long), cudaMemcpyDeviceToHost),
                            "batch times");
   if (rc) return rc;
-  for (int p = 0; p < np; ++p) ms[p] = (double)(t[p] - t[np]) * 1e-6;
+  for (int u = 0; u < B.nuser; ++u) ms[u] = 0.0;
+  for (int p = 0; p < np; ++p)  // a problem completes with its last pass
+    if (B.probs[p].next < 0) ms[B.probs[p].user] = (double)(t[p] - t[np]) * 1e-6;
   return MSB_OK;
 }
 
@@ -802,12 +856,13 @@ extern "C" int msb_batch_info(const msb_batch* b, msb_batch_info_t* info) {
   if (!b || !info) return msb::set_error(MSB_ERR_ARG, "batch: invalid argument");
   const BatchImpl& B = b->impl;
   memset(info, 0, sizeof *info);
-  info->nproblem = (int)B.probs.size();
+  info->nproblem = B.nuser;
   info->ntask = B.ntask;
   info->nclass = (int)B.classes.size();
   info->scratch_bytes = B.arena_bytes;
   size_t need = 0;
-  for (auto& p : B.probs) need += p.scratch;
+  for (auto& p : B.probs)
+    if (p.pass == 0) need += p.scratch;
   info->scratch_needed_all = need;
   info->npred = B.pred_off.empty() ? 0 : B.pred_off.back();
   info->nsm = B.nsm;
@@ -831,6 +886,17 @@ extern "C" long long msb_batch_tasks(const msb_batch* b, int* rec, int* prob, lo
   if (rec && m > 0) memcpy(rec, B.rec.data(), (size_t)m * MSB_TASK_INTS * sizeof(int));
   if (prob && m > 0) memcpy(prob, B.task_prob.data(), (size_t)m * sizeof(int));
   return B.ntask;
+}
+
+extern "C" int msb_batch_entries(const msb_batch* b, int* problem, int* angle0, int max_entries) {
+  if (!b) return msb::set_error(MSB_ERR_ARG, "batch: invalid argument");
+  const BatchImpl& B = b->impl;
+  const int ne = (int)B.probs.size();
+  for (int p = 0; p < ne && p < max_entries; ++p) {
+    if (problem) problem[p] = B.probs[p].user;
+    if (angle0) angle0[p] = B.probs[p].a0;
+  }
+  return ne;
 }
 
 extern "C" int msb_batch_scratch(const msb_batch* b, long long* offset, long long* bytes, int* pred_off, int* pred,

@@ -65,7 +65,10 @@ struct Fp64Prob {
   signed char sp_off;    // (ix_base + 3 iy_base) & 3 of a process's subdomain (KBA decomposition): the space
                          // factor (quantities_testing_kernels.h:97-126) takes global coordinates
   signed char pad_;
+  int a_stride;  // angles per octant row of afm / mfa (0: na); afm and mfa then point at the pass's first
+                 // angle of the caller's full matrices (a batch's angle passes read them in place)
 };
+static_assert(sizeof(Fp64Prob) == 96, "problem record size");
 
 // One problem per launch.
 struct Fp64Params {
@@ -309,16 +312,17 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
         if (failed) break;
         __threadfence_block();
         double* mat = mats + mb * C::MAT;
+        const size_t as = Q.a_stride ? (size_t)Q.a_stride : (size_t)Q.na;
         for (int e = lane; e < NCH * KS * 4 * 32; e += 32) {
           const int ln = e & 31, tt = (e >> 5) & 3, k = (e >> 7) % KS, ch = (e >> 7) / KS;
           const int ia = 32 * ch + 8 * tt + (ln >> 2), im = KS * (ln & 3) + k;
-          mat[e] = ia < Q.na ? __ldg(&Q.afm[ia + (size_t)Q.na * (im + (size_t)NM_ * oct)]) : 0.0;
+          mat[e] = ia < Q.na ? __ldg(&Q.afm[ia + as * (im + (size_t)NM_ * oct)]) : 0.0;
         }
         for (int e = lane; e < NCH * MT * 8 * 32; e += 32) {
           const int ln = e & 31, i = (e >> 5) & 1, tt = (e >> 6) & 3, mt = (e >> 8) % MT, ch = (e >> 8) / MT;
           const int ia = 32 * ch + 8 * tt + 2 * (ln & 3) + i, im = 8 * mt + (ln >> 2);
           mat[NCH * KS * 4 * 32 + e] =
-              (ia < Q.na && im < NM_) ? __ldg(&Q.mfa[im + (size_t)NM_ * (ia + (size_t)Q.na * oct)]) : 0.0;
+              (ia < Q.na && im < NM_) ? __ldg(&Q.mfa[im + (size_t)NM_ * (ia + as * oct)]) : 0.0;
         }
         if constexpr (BATCH) {
           if (lane == 0) s_prob[mb] = Q;  // published to the compute warps with the task's first stage
@@ -804,12 +808,11 @@ constexpr int batch_kind(int nm, int nch, bool tile24) {
 }
 
 // Every body kind of the batched kernel, in increasing kind order:
-// F(kind, NM, NCH, TX, TY).
+// F(kind, NM, NCH, TX, TY).  A batch sweeps its problems in 32-angle
+// entries, so only the one-chunk bodies are compiled.
 #define MSB_FP64_BATCH_KINDS(F)                                                                   \
-  F(BK_NM4_C1_42, 4, 1, 4, 2) F(BK_NM4_C1_24, 4, 1, 2, 4) F(BK_NM4_C2_42, 4, 2, 4, 2)             \
-  F(BK_NM4_C2_24, 4, 2, 2, 4) F(BK_NM8_C1_42, 8, 1, 4, 2) F(BK_NM8_C1_24, 8, 1, 2, 4)             \
-  F(BK_NM8_C2_42, 8, 2, 4, 2) F(BK_NM8_C2_24, 8, 2, 2, 4) F(BK_NM16_C1_42, 16, 1, 4, 2)           \
-  F(BK_NM16_C1_24, 16, 1, 2, 4) F(BK_NM16_C2_42, 16, 2, 4, 2) F(BK_NM16_C2_24, 16, 2, 2, 4)
+  F(BK_NM4_C1_42, 4, 1, 4, 2) F(BK_NM4_C1_24, 4, 1, 2, 4) F(BK_NM8_C1_42, 8, 1, 4, 2)             \
+  F(BK_NM8_C1_24, 8, 1, 2, 4) F(BK_NM16_C1_42, 16, 1, 4, 2) F(BK_NM16_C1_24, 16, 1, 2, 4)
 
 // Between two classes: every warp of the CTA is done with the previous
 // class's stages (a barrier that warps reach from their own role's code, so
@@ -875,11 +878,8 @@ template <int NS>
 constexpr size_t fp64_batch_smem() {
   size_t m = 0;
   const size_t v[] = {Fp64Cfg<4, 1, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<4, 1, 2, 4, NS>::smem_bytes_batch(),
-                      Fp64Cfg<4, 2, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<4, 2, 2, 4, NS>::smem_bytes_batch(),
                       Fp64Cfg<8, 1, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<8, 1, 2, 4, NS>::smem_bytes_batch(),
-                      Fp64Cfg<8, 2, 4, 2, NS>::smem_bytes_batch(),  Fp64Cfg<8, 2, 2, 4, NS>::smem_bytes_batch(),
-                      Fp64Cfg<16, 1, 4, 2, NS>::smem_bytes_batch(), Fp64Cfg<16, 1, 2, 4, NS>::smem_bytes_batch(),
-                      Fp64Cfg<16, 2, 4, 2, NS>::smem_bytes_batch(), Fp64Cfg<16, 2, 2, 4, NS>::smem_bytes_batch()};
+                      Fp64Cfg<16, 1, 4, 2, NS>::smem_bytes_batch(), Fp64Cfg<16, 1, 2, 4, NS>::smem_bytes_batch()};
   for (size_t x : v) m = x > m ? x : m;
   return m;
 }

@@ -3,12 +3,15 @@
 A batch sweeps many problems in one persistent launch.  Its task table must
 be safe for the kernel's protocol:
 
+* every problem is swept in entries of 32 angles (its angle passes), in
+  pass order: each later pass shares the first pass's scratch and waits for
+  the pass before it;
 * topological: every dependency of a task precedes it in the table, and
-  belongs to the same problem;
+  belongs to the same entry;
 * one contiguous range per class (the CTAs work through classes in order);
-* every problem's tasks are exactly the schedule its own Sweeper would build
-  for the same tile (the per-problem records, dependencies renumbered);
-* face scratch: two problems whose arena ranges overlap are ordered -- all
+* every entry's tasks are exactly the schedule its problem's own Sweeper
+  would build for the same tile (the records, dependencies renumbered);
+* face scratch: two entries whose arena ranges overlap are ordered -- all
   tasks of the earlier one precede all tasks of the later one in the table,
   and the later one waits (transitively) for the earlier one's completion.
 """
@@ -40,7 +43,13 @@ def check_plan(b, problems, mask=0):
     rec, prob = b.tasks()
     n = len(rec)
     info = b.info()
-    assert info["ntask"] == n
+    assert info["ntask"] == n and info["nproblem"] == len(problems)
+    eprob, ea0 = b.entries()
+    # entries: every problem's 32-angle passes, in order
+    for p, pr in enumerate(problems):
+        mine = np.nonzero(eprob == p)[0]
+        assert list(ea0[mine]) == list(range(0, pr["na"], 32))
+        assert np.all(np.diff(mine) == 1)
     idx = np.arange(n)
     # topological, same-problem dependencies
     for d in DEPS:
@@ -53,14 +62,14 @@ def check_plan(b, problems, mask=0):
     for c in info["classes"]:
         total += c["ntask"]
     assert total == n
-    change = np.count_nonzero(np.diff([_class_of(problems[p], info) for p in prob]))
+    change = np.count_nonzero(np.diff([_class_of(problems[eprob[e]], info) for e in prob]))
     assert change <= info["nclass"] - 1
-    # each problem's records = its own schedule (dependencies renumbered)
-    for p, pr in enumerate(problems):
-        mine = np.nonzero(prob == p)[0]
-        nch = (pr["na"] + 31) // 32
+    # each entry's records = its problem's own schedule (dependencies renumbered)
+    for e in range(len(eprob)):
+        pr = problems[eprob[e]]
+        mine = np.nonzero(prob == e)[0]
         k = {4: 0, 8: 1, 16: 2}[pr["nm"]]
-        t24 = (mask >> (3 * (nch - 1) + k)) & 1
+        t24 = (mask >> k) & 1
         tx, ty = (2, 4) if t24 else (4, 2)
         own = msb.schedule(pr["ncell_x"], pr["ncell_y"], pr["ncell_z"], pr["ne"], tx, ty, 1)
         assert len(own) == len(mine)
@@ -82,9 +91,8 @@ def check_plan(b, problems, mask=0):
 
 
 def _class_of(p, info):
-    nch = (p["na"] + 31) // 32
     for c, cl in enumerate(info["classes"]):
-        if cl["nm"] == p["nm"] and cl["nch"] == nch:
+        if cl["nm"] == p["nm"] and cl["nch"] == 1:
             return c
     raise AssertionError("no class")
 
@@ -93,10 +101,20 @@ def test_plan_all_resident():
     b = plan(SMALL)
     check_plan(b, SMALL)
     off, nb, po, pred = b.scratch()
-    assert len(pred) == 0  # enough scratch for all at once: no waiting
-    # disjoint placement
-    order = np.argsort(off)
-    assert np.all(off[order][1:] >= (off + nb)[order][:-1])
+    eprob, ea0 = b.entries()
+    # enough scratch for all at once: an entry waits only for its problem's
+    # previous pass, whose scratch it shares
+    for e in range(len(eprob)):
+        ps = list(pred[po[e]:po[e + 1]])
+        if ea0[e] == 0:
+            assert ps == []
+        else:
+            assert ps == [e - 1] and eprob[e - 1] == eprob[e] and off[e] == off[e - 1]
+    # the problems' placements are disjoint
+    first = ea0 == 0
+    order = np.argsort(off[first])
+    o, b_ = off[first][order], (off + nb)[first][order]
+    assert np.all(o[1:] >= b_[:-1])
 
 
 @pytest.mark.parametrize("mask", [0, 0b111111, 0b101010])
@@ -113,9 +131,10 @@ def test_plan_reuse_is_ordered(nsm):
     b = plan(SMALL, nsm=nsm, scratch=int(nb.max()))
     rec, prob = check_plan(b, SMALL)
     off, nb, po, pred = b.scratch()
-    first = np.array([np.min(np.nonzero(prob == p)[0]) for p in range(len(SMALL))])
-    last = np.array([np.max(np.nonzero(prob == p)[0]) for p in range(len(SMALL))])
-    preds = [set(pred[po[p]:po[p + 1]]) for p in range(len(SMALL))]
+    n = len(off)  # entries
+    first = np.array([np.min(np.nonzero(prob == p)[0]) for p in range(n)])
+    last = np.array([np.max(np.nonzero(prob == p)[0]) for p in range(n)])
+    preds = [set(pred[po[p]:po[p + 1]]) for p in range(n)]
 
     def waits_for(q, p):  # q waits (transitively) for p
         seen, todo = set(), [q]
@@ -129,7 +148,6 @@ def test_plan_reuse_is_ordered(nsm):
                     todo.append(y)
         return False
 
-    n = len(SMALL)
     overlaps = 0
     for p in range(n):
         for q in range(n):
@@ -153,7 +171,7 @@ def test_plan_scratch_too_small():
 
 def test_plan_rejects_unsupported():
     with pytest.raises(msb.SweepError):
-        plan([dict(ncell_x=2, ncell_y=2, ncell_z=2, ne=2, na=65, nm=16)])
+        plan([dict(ncell_x=2, ncell_y=2, ncell_z=2, ne=2, na=129, nm=16)])
     with pytest.raises(msb.SweepError):
         plan([dict(ncell_x=2, ncell_y=2, ncell_z=2, ne=2, na=16, nm=12)])
     with pytest.raises(msb.SweepError):
