@@ -175,3 +175,64 @@ def test_decomposed_refuses_other_kernels():
     with pytest.raises(msb.SweepError) as e:
         msb.Problem(common + " --precision 1", nm=16, proc=0, nproc=2, comm=comm)
     assert e.value.code == msb.MSB_ERR_UNSUPPORTED
+
+
+# ------------------------------------- the torch.distributed transport, 2 processes
+def _torch_rank(rank, world, port, common, npx, npy, nm, out):
+    import datetime
+    import os
+
+    import torch.distributed as dist
+
+    from minisweep_b200.parallel import TorchGroupComm
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        tg = TorchGroupComm()
+        args = f"{common} --nproc_x {npx} --nproc_y {npy} --nblock_z 2"
+        with msb.Problem(args, nm=nm, proc=rank, nproc=world, comm=tg.comm) as pb:
+            # both processes drive this one GPU: their sweep kernels take turns
+            pb.env.flags_ |= 1
+            tg.attach(pb)
+            vi = pb.init_state()
+            vo = pb.sweep_host(vi)          # Sweeper_sweep: the library's step loop and the callbacks
+            n2, d2 = pb.state_norms(vi, vo)  # Env_sum_P over the group
+            out[rank] = (pb.x0, pb.y0, pb.dims.ncell_x, pb.dims.ncell_y, vo, n2, d2)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("npx,npy", [(2, 1), (1, 2)])
+def test_torch_group_transport(npx, npy):
+    import socket
+
+    import torch.multiprocessing as mp
+
+    common = "--ncell_x 7 --ncell_y 6 --ncell_z 4 --ne 3 --na 40"
+    nm = 16
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    with mp.Manager() as man:
+        out = man.dict()
+        mp.start_processes(_torch_rank, args=(2, port, common, npx, npy, nm, out), nprocs=2, join=True,
+                           start_method="spawn")
+        res = dict(out)
+    vi = init_global(common, nm)
+    ref = sweep_single(common, nm, vi)
+    kv = _parse(common)
+    gx, gy, nz, ne = kv["--ncell_x"], kv["--ncell_y"], kv["--ncell_z"], kv["--ne"]
+    got = np.zeros((nz, ne, gy, gx, msb.NU, nm))
+    for r in range(2):
+        x0, y0, nx, ny, vo, n2, d2 = res[r]
+        got[:, :, y0:y0 + ny, x0:x0 + nx] = vo.reshape(nz, ne, ny, nx, msb.NU, nm)
+        assert d2 == 0.0
+    assert np.array_equal(got.reshape(-1), ref)
+    with msb.Problem(common, nm=nm) as pb:
+        n1, _ = pb.state_norms(vi, ref)
+    assert all(res[r][5] == n1 for r in range(2))
