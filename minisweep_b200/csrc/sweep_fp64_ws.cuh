@@ -156,7 +156,8 @@ struct Fp64Cfg {
   static constexpr int SM_FINAL = SM_BAR + 3 * NS;      // loader -> publisher: steps issued (int)
   static constexpr int SM_PROB = SM_FINAL + 1;          // batched: Fp64Prob of the task in each mat buffer
   static constexpr size_t smem_bytes() { return sizeof(double) * (size_t)SM_PROB; }
-  static constexpr size_t smem_bytes_batch() { return sizeof(double) * (size_t)SM_PROB + 2 * sizeof(Fp64Prob); }
+  // batched: two problem records, then the problem whose predecessors the loader last saw complete (int)
+  static constexpr size_t smem_bytes_batch() { return sizeof(double) * (size_t)SM_PROB + 2 * sizeof(Fp64Prob) + 16; }
 };
 
 // Shared-memory barriers of one body: set up before its first stage, and
@@ -221,6 +222,11 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
       long long g_load = 0;
       long long last_step[2] = {-1, -1};  // last global step of the task using mat buffer 0/1
       int ntask_seen = 0;
+      // BATCH: the problem whose predecessors were last seen complete (kept
+      // in shared memory: the producer warps' registers are all in use)
+      volatile int* const preds_done_for = reinterpret_cast<volatile int*>(s_prob + 2);
+      if (BATCH && lane == 0) *preds_done_for = -1;
+      __syncwarp();
       bool failed = false;
 
       // Steps up to freed_upto have been consumed by the publisher.  Waiting
@@ -294,9 +300,15 @@ __device__ __forceinline__ void fp64_body(const PP& P, int cls) {
             Q.vo = const_cast<double*>(a);
           }
           // the face scratch is free once its previous users completed
-          for (int k = __ldg(&P.pred_off[prob]), ke = __ldg(&P.pred_off[prob + 1]); k < ke && !failed; ++k) {
-            const int q2 = __ldg(&P.pred[k]);
-            if (wait_dep(&P.pdone[q2], __ldg(&P.prob_ntask[q2]), t) < 0) failed = true;
+          // (completion is final: checked once per run of tasks of one problem)
+          if (prob != *preds_done_for) {
+            for (int k = __ldg(&P.pred_off[prob]), ke = __ldg(&P.pred_off[prob + 1]); k < ke && !failed; ++k) {
+              const int q2 = __ldg(&P.pred[k]);
+              if (wait_dep(&P.pdone[q2], __ldg(&P.prob_ntask[q2]), t) < 0) failed = true;
+            }
+            __syncwarp();
+            if (!failed && lane == 0) *preds_done_for = prob;
+            __syncwarp();
           }
         } else {
           Q = P.pr;
