@@ -18,9 +18,10 @@
 //   FP16 halves that is a 22-bit significand per operand (errors near FP32
 //   rounding); with BF16 halves 16 bits.  Quantities_solve
 //   (quantities_testing_kernels.h:337-447) runs in FP32 with fused
-//   multiply-adds except its last step, psi = sm * cc + vs, which is formed
-//   in FP64 (with the FP64 reciprocal 1 / (1 + octant)) and rounded once to
-//   FP32; faces are stored in FP32.  vo is read, summed and written in FP64.
+//   multiply-adds except its last step, psi = sm * cc + vs, which carries
+//   the FP64 reciprocal 1 / (1 + octant) as an FP32 pair and the product's
+//   and the sum's rounding errors (fma, TwoSum) to one final rounding;
+//   faces are stored in FP32.  vo is summed and written in FP64.
 //
 // Tile and roles (one CTA, 10 warps)
 //   A task is a 4 x 4 tile of cell columns x one group pair.  MMA row
@@ -669,9 +670,12 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const int cbeg = a + b;
       const int kb1 = mat_scale[2 * mb], kb2 = mat_scale[2 * mb + 1];
       const float so = (float)(1 + oct);
-      // 1 / (1 + octant) rounded in FP64, as the reference rounds it: the
-      // product with it is formed in FP64 (see the solve below)
+      // 1 / (1 + octant) rounded in FP64, as the reference rounds it, carried
+      // as an FP32 pair so_hi + so_lo (to 2^-48): the solve forms its product
+      // with psi's other terms with one final rounding (see below)
       const double so_rd = 1.0 / (double)(1 + oct);
+      const float so_hi = __double2float_rn(so_rd);
+      const float so_lo = __double2float_rn(so_rd - (double)so_hi);
       const float face_k =
           rowv ? (float)d_scale_energy(P.ie_base + g_col) * (float)d_scale_unknown(u) * so : 0.0f;
       const int sp_xy = ix + 3 * iy + 2;
@@ -744,17 +748,19 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         tmem_ld8(trow + C::TM_D2 + (uint32_t)(pe.gg & 1) * 32 + 16 + MH * half, d1);
         tmem_wait_ld();
         if (pe.act) {
-          // un-scale in FP64: exact, and no intermediate can overflow (the
-          // scaled accumulators times 2^-k may exceed the FP32 range even
-          // where the result does not)
+          // un-scale: each accumulator times 2^e with e = -k2 - kb2 (|e| <=
+          // 240) in two exact power-of-two steps of e / 2 (an intermediate
+          // lies between the accumulator and the result, so it stays normal
+          // wherever both do), the two halves' terms added with one
+          // rounding (fma)
           const int kx = (pe.gg & 1) * 256 + row;
-          // un-scaled in FP64 (exact; no intermediate can overflow), rounded
-          // once to FP32
-          const double s0 = d_pow2(-k2s[kx] - kb2), s1 = d_pow2(-k2s[kx + 128] - kb2);
+          const int e0 = -k2s[kx] - kb2, e1 = -k2s[kx + 128] - kb2;
+          const float f0a = f_pow2(e0 / 2), f0b = f_pow2(e0 - e0 / 2);
+          const float f1a = f_pow2(e1 / 2), f1b = f_pow2(e1 - e1 / 2);
           float o[MH];
 #pragma unroll
           for (int m = 0; m < MH; ++m)
-            o[m] = __double2float_rn(__fma_rn((double)d0[m], s0, __dmul_rn((double)d1[m], s1)));
+            o[m] = __fmaf_rn(__fmul_rn(d0[m], f0a), f0b, __fmul_rn(__fmul_rn(d1[m], f1a), f1b));
           float* dst = pe.dst + MH * half;
           if constexpr (MH % 4 == 0) {
 #pragma unroll
@@ -805,7 +811,8 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         const float cxy = f_pow2(-1 - ((sp_xy + 7 * (iz - dz)) & 3));
         const float cxz = f_pow2(-2 - ((sp_xy - 3 * dy + 7 * iz) & 3));
         const float sx_r = f_pow2(-((sp_xy - dx + 7 * iz) & 3));
-        const double ccd = so_rd * d_pow2((sp_xy + 7 * iz) & 3);
+        const float ccp = f_pow2((sp_xy + 7 * iz) & 3);  // exact scalings of so_hi / so_lo
+        const float cch = __fmul_rn(so_hi, ccp), ccl = __fmul_rn(so_lo, ccp);
         // vs = D1a * 2^-(k1 + kb1) [+ D1b * 2^-(k1b + kb1)], each term in two
         // exact steps, the smaller factor first, so no intermediate leaves the
         // FP32 range unless the term itself does
@@ -878,12 +885,20 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
             const float sm = __fmaf_rn(fyz[i], __fmul_rn(wz, sx_r), sab);
             float vs = __fmul_rn(__fmul_rn(v[i], vsc1), vsc2);
             if constexpr (C::SPLIT_K) vs = __fmaf_rn(__fmul_rn(vb[i], vbs1), vbs2, vs);
-            // psi = sm * cc + vs with one rounding from FP64: the FP64
-            // reciprocal of (1 + octant) and no FP32 rounding of the product
-            // (formed in FP32 -- with the FP32 reciprocal and product -- the
-            // cancellation of the large boundary fluxes in T2 amplifies that
-            // rounding up to 1e-4 relative in vo at na 64-128)
-            const float psi = __double2float_rn(__fma_rn((double)sm, ccd, (double)vs));
+            // psi = sm * cc + vs rounded once to FP32, with cc the FP64
+            // reciprocal of (1 + octant) as cch + ccl: the product's
+            // rounding error (fma), the sum's (TwoSum) and the low part
+            // are added back before the final rounding.  (With the FP32
+            // reciprocal and a rounded product, the cancellation of the
+            // large boundary fluxes in T2 amplified that rounding up to
+            // 1e-4 relative in vo at na 64-128.)  FP32 operations only; the
+            // same sum formed in FP64 and rounded took 1 % more time.
+            const float pp = __fmul_rn(sm, cch);
+            const float pl = __fmaf_rn(sm, ccl, __fmaf_rn(sm, cch, -pp));
+            const float s2 = __fadd_rn(pp, vs);
+            const float bb = __fsub_rn(s2, pp);
+            const float er = __fadd_rn(__fsub_rn(pp, __fsub_rn(s2, bb)), __fsub_rn(vs, bb));
+            const float psi = __fadd_rn(s2, __fadd_rn(er, pl));
             v[i] = psi;
             pmax = fmaxf(pmax, fabsf(psi));
             carry[i] = __fmul_rn(psi, so);
