@@ -63,15 +63,14 @@
 
 namespace msb {
 
-// tm_vi describes the state array as a 5-D tensor (moment, NU * x, y, group,
-// z) for TMA tile copies of one cell: a box of NM moments x 4 unknowns x 1 x 2
-// groups x 1, swizzled so that rows read by consecutive lanes fall in
-// distinct banks.  Each octant's contribution to vo is written to its own
-// FP32 partial array (the state layout, `part + oct * state`); a second
-// kernel sums the eight partials into vo in FP64.
+// vi16 holds the sweep's input state converted once per sweep into the first
+// transform's operand format (convert_vi16 below): one block of kViBlock
+// bytes per (cell, group pair), copied whole into a stage by the loader.
+// Each octant's contribution to vo is written to its own FP32 partial array
+// (the state layout, `part + oct * state`); a second kernel sums the eight
+// partials into vo in FP64.
 struct MixParams {
-  CUtensorMap tm_vi;
-  const double* vi;
+  const unsigned char* vi16;
   float* part;
   size_t state;  // elements of one state array
   const double* afm;  // a_from_m [oct][im][ia]
@@ -84,9 +83,15 @@ struct MixParams {
   int nx, ny, nz, ne, na, ngp;
   int ia_base;     // angle index of the first angle of afm / mfa (32-angle passes over a larger na)
   int ie_base;     // global index of group 0 (energy-group slices of a larger problem)
-  int vbox_bytes;  // bytes one TMA box delivers (both groups; one group when ne == 1)
   SyncArgs sy;
 };
+
+// One (cell, group pair) of vi in the first transform's operand format: the
+// cell's 8 rows (group g, unknown u: row 4 g + u) of A1, hi halves then lo
+// halves, each 256 bytes in the K-major core-matrix order of A1 ([moment
+// chunk 8 m / 8][row][moment % 8], 2 bytes each), then the row scale 2^k1
+// of each (moment chunk, row) as one signed byte.
+constexpr int kViBlock = 2 * 256 + 16;
 
 enum MixFormat { MIX_F16 = 0, MIX_BF16 = 1 };
 
@@ -201,22 +206,16 @@ struct MixCfg {
   static constexpr int KP = 16;             // moments, padded to one MMA K-step
   static constexpr int NA = 32;             // angles per MMA: one pass (larger na: one pass per 32)
   static constexpr int EB = 1024;           // bytes per face entry: 8 rows x 32 floats
-  // vi / previous-vo blocks: 128 rows of NM doubles; one cell (2 groups x 4
-  // unknowns = 8 rows) is one TMA box, swizzled: the 16-byte chunk j of row r
-  // sits at chunk j ^ ((r * VROW / 128) & SWM) of its 128-byte segment
-  static constexpr int VROW = NM_ * 8;
-  static constexpr int VCELL = 8 * VROW;  // bytes of one box (alignment of its destination)
-  static constexpr int VBUF = 128 * VROW;
-  static constexpr int SWM = NM_ == 16 ? 7 : NM_ == 8 ? 3 : 1;
   // stage (bytes), filled by the loader with bulk copies: entering yz faces
   // (one per tile row), xz (one per column), xy of the first plane (one per
-  // row), vi of every cell column at this step, then the step header
+  // row), the vi16 block of every cell column at this step, then the step
+  // header
   static constexpr int ST_YZ = 0;
   static constexpr int ST_XZ = ST_YZ + TY * EB;
   static constexpr int ST_XY = ST_XZ + TX * EB;
   static constexpr int ST_VI = ST_XY + TY * EB;
-  static constexpr int ST_HDR = ST_VI + VBUF;
-  static constexpr int STAGE = (ST_HDR + 128 + 1023) / 1024 * 1024;  // keeps every vi box 1 KiB aligned
+  static constexpr int ST_HDR = ST_VI + TX * TY * kViBlock;
+  static constexpr int STAGE = (ST_HDR + 128 + 1023) / 1024 * 1024;
   // MMA operands (bytes); each comes as a hi and a lo matrix
   static constexpr int A1M = 128 * KP * 2;  // LBO 128, SBO 256
   static constexpr int A2M = 128 * NA * 2;  // LBO 128, SBO 512
@@ -244,13 +243,6 @@ struct MixCfg {
   static constexpr int TM_COLS = 256;
   static constexpr int TM_D1 = 0, TM_D2 = 128;
 };
-
-// Byte offset of (row, 16-byte chunk jj) in a swizzled vi / vo block buffer.
-template <class C>
-__device__ __forceinline__ int vswz(int row, int jj) {
-  const int r = row * C::VROW;
-  return r + ((16 * jj) ^ (((r >> 7) & C::SWM) << 4));
-}
 
 template <int NM_, int FMT, int NS>
 __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(const __grid_constant__ MixParams P) {
@@ -444,7 +436,7 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         // vi of cell (va, vb), both groups, at this step: lane 4*vb + va
         const int va = lane & 3, vb = lane >> 2, cvi = s - va - vb;
         const bool vi_ok = lane < TX * TY && va < w && vb < h && cvi >= 0 && cvi < nzr;
-        uint32_t bytes = (uint32_t)__popc(__ballot_sync(0xffffffffu, vi_ok)) * P.vbox_bytes;
+        uint32_t bytes = (uint32_t)__popc(__ballot_sync(0xffffffffu, vi_ok)) * (uint32_t)kViBlock;
         for (int b = 0; b < h; ++b) {
           const int c = s - b;
           if ((flags & TF_X_IN) && c >= 0 && c < nzr) bytes += EB;
@@ -465,7 +457,9 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
         if (vi_ok) {
           const int ix = dx > 0 ? x0 + va : x1 - 1 - va, iy = dy > 0 ? y0 + vb : y1 - 1 - vb;
           const int iz = dz > 0 ? z0 + cvi : z1 - 1 - cvi;
-          tma_load_5d(stg + C::ST_VI + (4 * vb + va) * C::VCELL, &P.tm_vi, 0, NU * ix, iy, 2 * gp, iz, &full[st]);
+          bulk_g2s(stg + C::ST_VI + (4 * vb + va) * kViBlock,
+                   P.vi16 + (((size_t)iz * P.ngp + gp) * P.ny * P.nx + (size_t)iy * P.nx + ix) * kViBlock, kViBlock,
+                   &full[st]);
         }
         // lanes [0, TY): yz of row b; [8, 8+TX): xz of column a; [16, 16+TY): xy of row b
         const int kind = lane >> 3, pos = lane & 7;
@@ -693,40 +687,17 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
       const long long zstep = (long long)(slab * P.ne) * dz;
       float* const part_oct = P.part + P.state * (size_t)oct;
 
-      // vi of global step gg (landed in its stage) -> scaled hi/lo K-chunk
-      // `half` of this row of A1 (moments 8*half .. 8*half + 7, zero padded)
+      // vi of global step gg (its vi16 block landed in its stage) -> K-chunk
+      // `half` of this row of A1, hi and lo, and the chunk's row scale
       auto convert_vi = [&](long long gg, bool act) {
         int k1 = 0;
-        uint32_t hi[4] = {0u, 0u, 0u, 0u}, lo[4] = {0u, 0u, 0u, 0u};
-        constexpr int M0 = 0;  // first moment of the chunk, relative to 8 * half
-        if (act && 8 * half < NM_) {
-          const unsigned char* src = stages + (size_t)(gg % NS) * C::STAGE + C::ST_VI;
-          constexpr int NMC = NM_ < 8 ? NM_ : 8;  // moments in this chunk
-          double v[NMC];
-#pragma unroll
-          for (int jj = 0; jj < NMC / 2; ++jj) {
-            const double2 p = *reinterpret_cast<const double2*>(src + vswz<C>(row, 4 * half + jj));
-            v[2 * jj] = p.x;
-            v[2 * jj + 1] = p.y;
-          }
-          int emax = 0;  // largest biased exponent of the chunk
-#pragma unroll
-          for (int k = 0; k < NMC; ++k) emax = max(emax, (int)((__double_as_longlong(v[k]) >> 52) & 0x7ff));
-          k1 = emax == 0 ? 0 : max(-120, min(120, 15 - (emax - 1022)));
-          const double sc = d_pow2(k1);
-#pragma unroll
-          for (int p = 0; p < 4; ++p) {
-            const float x0 = M0 + 2 * p < NMC ? __double2float_rn(v[2 * p < NMC ? 2 * p : 0] * sc) : 0.0f;
-            const float x1 = M0 + 2 * p + 1 < NMC ? __double2float_rn(v[2 * p + 1 < NMC ? 2 * p + 1 : 0] * sc) : 0.0f;
-            hi[p] = H::pack(x0, x1);
-            const float2 hv = H::unpack(hi[p]);
-            lo[p] = H::pack(__fsub_rn(x0, hv.x), __fsub_rn(x1, hv.y));
-          }
-        }
         if (act) {
+          const unsigned char* blk = stages + (size_t)(gg % NS) * C::STAGE + C::ST_VI + (row >> 3) * kViBlock;
+          const int o = half * 128 + (row & 7) * 16;
           const int off = kmajor_off(row, 8 * half, 128, 256);
-          *reinterpret_cast<uint4*>(a1s + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<uint4*>(a1s + C::A1M + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          *reinterpret_cast<uint4*>(a1s + off) = *reinterpret_cast<const uint4*>(blk + o);
+          *reinterpret_cast<uint4*>(a1s + C::A1M + off) = *reinterpret_cast<const uint4*>(blk + 256 + o);
+          k1 = (int)reinterpret_cast<const signed char*>(blk + 512)[half * 8 + (row & 7)];
         }
         k1s[(gg & 1) * 256 + half * 128 + row] = k1;
       };
@@ -972,6 +943,60 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
   tc_fence_after();
   if (warp == NW + 2)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TM_COLS) : "memory");
+}
+
+// vi -> vi16, once per sweep: thread t converts moment chunk `half` (moments
+// 8 half .. 8 half + 7, zero padded) of row r8 = 4 g + u of block t / 16
+// (cell (ix, iy, iz), group pair gp; group 2 gp + g, unknown u).  The chunk
+// is scaled by 2^k1 so that its largest entry lies in [2^14, 2^15) (k1
+// clamped to [-120, 120]), rounded to FP32 in FP64 and split into hi + lo
+// 16-bit halves -- the operand every octant's first transform of that cell
+// uses.  A group beyond ne (odd ne) and the chunks beyond NM are zeros.
+template <int NM_, int FMT>
+__global__ void __launch_bounds__(256) convert_vi16(const double* __restrict__ vi, unsigned char* __restrict__ out,
+                                                    int nx, int ny, int nz, int ne, int ngp) {
+  using H = Half16<FMT>;
+  constexpr int NMC = NM_ < 8 ? NM_ : 8;  // moments of a chunk
+  const long long nunit = (long long)nx * ny * nz * ngp * 16;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nunit;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int r8 = (int)(t & 7), half = (int)((t >> 3) & 1);
+    const long long blk = t >> 4;
+    const int ix = (int)(blk % nx);
+    long long q = blk / nx;
+    const int iy = (int)(q % ny);
+    q /= ny;
+    const int gp = (int)(q % ngp), iz = (int)(q / ngp);
+    const int g = r8 >> 2, u = r8 & 3, ie = 2 * gp + g;
+    int k1 = 0;
+    uint32_t hi[4] = {0u, 0u, 0u, 0u}, lo[4] = {0u, 0u, 0u, 0u};
+    if (ie < ne && 8 * half < NM_) {
+      const double* src =
+          vi + (size_t)NM_ * (u + (size_t)NU * (ix + (size_t)nx * (iy + (size_t)ny * (ie + (size_t)ne * iz)))) +
+          8 * half;
+      double v[NMC];
+#pragma unroll
+      for (int k = 0; k < NMC; ++k) v[k] = __ldcs(src + k);
+      int emax = 0;  // largest biased exponent of the chunk
+#pragma unroll
+      for (int k = 0; k < NMC; ++k) emax = max(emax, (int)((__double_as_longlong(v[k]) >> 52) & 0x7ff));
+      k1 = emax == 0 ? 0 : max(-120, min(120, 15 - (emax - 1022)));
+      const double sc = d_pow2(k1);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const float x0 = 2 * p < NMC ? __double2float_rn(v[2 * p < NMC ? 2 * p : 0] * sc) : 0.0f;
+        const float x1 = 2 * p + 1 < NMC ? __double2float_rn(v[2 * p + 1 < NMC ? 2 * p + 1 : 0] * sc) : 0.0f;
+        hi[p] = H::pack(x0, x1);
+        const float2 hv = H::unpack(hi[p]);
+        lo[p] = H::pack(__fsub_rn(x0, hv.x), __fsub_rn(x1, hv.y));
+      }
+    }
+    unsigned char* b = out + (size_t)blk * kViBlock;
+    const int o = half * 128 + r8 * 16;
+    *reinterpret_cast<uint4*>(b + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(b + 256 + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    reinterpret_cast<signed char*>(b + 512)[half * 8 + r8] = (signed char)k1;
+  }
 }
 
 // vo = sum over the eight octants of their FP32 partials, in FP64 and in

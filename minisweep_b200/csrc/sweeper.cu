@@ -26,11 +26,13 @@ namespace {
 
 using KernelFn = void (*)(const Fp64Params);
 using MixKernelFn = void (*)(const MixParams);
+using MixConvFn = void (*)(const double*, unsigned char*, int, int, int, int, int);
 
 // One compiled kernel: the FP64 kernel (fn) or a mixed-precision one (mix).
 struct Variant {
   KernelFn fn = nullptr;
   MixKernelFn mix = nullptr;
+  MixConvFn conv = nullptr;  // mixed precision: vi into the first transform's operand format
   size_t smem = 0;
   size_t entry_bytes = 0;  // one face entry (octant, group pair, position)
   int tx = 0, ty = 0, nch = 0, threads = 0;
@@ -101,6 +103,7 @@ Variant make_mixed() {
   static_assert(C::smem_bytes() + 128 <= 227 * 1024, "shared memory budget (dynamic + static)");
   Variant v;
   v.mix = sweep_mixed_kernel<NM_, FMT, kMixStages>;
+  v.conv = convert_vi16<NM_, FMT>;
   v.smem = C::smem_bytes();
   v.entry_bytes = C::EB;
   v.tx = C::TX;
@@ -155,49 +158,6 @@ Variant pick_variant(int nm, int na, int precision, int tile = 0, int kernel = 0
     case 16: return pick_nch<16>(nch, tile);
     default: return Variant();
   }
-}
-
-// cuTensorMapEncodeTiled from the driver, through the runtime (no -lcuda).
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
-  return fn;
-}
-
-// The state array (im fastest, then iu, ix, iy, ie, iz) as a 5-D tensor
-// (moment, unknown * x, y, group, z) whose box is one cell: NM moments x 4
-// unknowns x 1 x (2 groups, 1 when ne == 1) x 1, copied with the swizzle the
-// mixed kernel reads with.
-int encode_state_map(CUtensorMap* map, const double* ptr, const Dimensions& d, int* box_bytes) {
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (!enc) return set_error(MSB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  if (reinterpret_cast<uintptr_t>(ptr) % 16 != 0)
-    return set_error(MSB_ERR_ARG, "the mixed-precision sweep needs 16-byte aligned state arrays");
-  const cuuint64_t row = (cuuint64_t)d.nm * sizeof(double);
-  const cuuint64_t dims[5] = {(cuuint64_t)d.nm, (cuuint64_t)NU * d.ncell_x, (cuuint64_t)d.ncell_y, (cuuint64_t)d.ne,
-                              (cuuint64_t)d.ncell_z};
-  const cuuint64_t strides[4] = {row, row * NU * d.ncell_x, row * NU * d.ncell_x * d.ncell_y,
-                                 row * NU * d.ncell_x * d.ncell_y * d.ne};
-  const cuuint32_t ng = d.ne >= 2 ? 2 : 1;
-  const cuuint32_t box[5] = {(cuuint32_t)d.nm, (cuuint32_t)NU, 1, ng, 1};
-  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-  const CUtensorMapSwizzle swz = d.nm == 16 ? CU_TENSOR_MAP_SWIZZLE_128B
-                                 : d.nm == 8 ? CU_TENSOR_MAP_SWIZZLE_64B
-                                             : CU_TENSOR_MAP_SWIZZLE_32B;
-  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double*>(ptr), dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return set_error(MSB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  *box_bytes = (int)(d.nm * sizeof(double) * NU * ng);
-  return MSB_OK;
 }
 
 }  // namespace
@@ -256,6 +216,7 @@ struct SweeperImpl {
   double* d_afm = nullptr;
   double* d_mfa = nullptr;
   float* d_part = nullptr;  // mixed precision: FP32 partial vo per octant
+  unsigned char* d_vi16 = nullptr;  // mixed precision: vi in the first transform's operand format
   size_t part_elems = 0;
   double* d_afm_c = nullptr;  // na above one pass: the pass's angle range of each matrix
   double* d_mfa_c = nullptr;
@@ -285,6 +246,7 @@ struct SweeperImpl {
     cudaFree(d_afm);
     cudaFree(d_mfa);
     cudaFree(d_part);
+    cudaFree(d_vi16);
     cudaFree(d_afm_c);
     cudaFree(d_mfa_c);
     cudaFree(d_vi);
@@ -396,6 +358,8 @@ static int impl_create(SweeperImpl& S, const Dimensions& dims, int precision, in
     S.part_elems = (size_t)NOCTANT * Dimensions_size_state(dims, NU);
     if ((rc = cuda_check(cudaMalloc(&S.d_part, S.part_elems * sizeof(float)), "cudaMalloc octant partials")))
       return rc;
+    const size_t nvi16 = (size_t)dims.ncell_x * dims.ncell_y * dims.ncell_z * S.ngp * kViBlock;
+    if ((rc = cuda_check(cudaMalloc(&S.d_vi16, nvi16), "cudaMalloc converted vi"))) return rc;
   }
   const size_t nmat = (size_t)dims.nm * dims.na * NOCTANT;
   if ((rc = cuda_check(cudaMalloc(&S.d_afm, nmat * sizeof(double)), "cudaMalloc a_from_m"))) return rc;
@@ -438,7 +402,8 @@ static int reset_pass(SweeperImpl& S, cudaStream_t stream) {
 // Problem fields (X) and schedule fields (P) of a launch; F is the face type.
 template <class F, class X, class PP>
 static void fill_params(const SweeperImpl& S, X& x, PP& P, const double* vi_d, const int* d_tasks, long long ntask) {
-  x.vi = vi_d;
+  if constexpr (std::is_same<X, Fp64Prob>::value) x.vi = vi_d;  // the mixed sweep reads vi16 instead
+  else (void)vi_d;
   x.afm = S.d_afm;
   x.mfa = S.d_mfa;
   x.fxy = static_cast<F*>(S.d_face[0]);
@@ -496,7 +461,11 @@ static int launch_mixed(SweeperImpl& S, double* vo_d, const double* vi_d, cudaSt
   P.part = S.d_part;
   P.state = S.part_elems / NOCTANT;
   int rc;
-  if ((rc = encode_state_map(&P.tm_vi, vi_d, S.dims, &P.vbox_bytes))) return rc;
+  // vi in the first transform's operand format, once for every octant and pass
+  S.var.conv<<<S.nsm * 8, 256, 0, stream>>>(vi_d, S.d_vi16, S.dims.ncell_x, S.dims.ncell_y, S.dims.ncell_z,
+                                            S.dims.ne, S.ngp);
+  if ((rc = cuda_check(cudaGetLastError(), "vi conversion launch"))) return rc;
+  P.vi16 = S.d_vi16;
   for (int c = 0; c < npass; ++c) {
     if (npass > 1) {
       const int a0 = pa * c, nac = std::min(pa, na - a0);
