@@ -319,8 +319,9 @@ def measure_mixed(args, pb64, flags, va, vb, stream, dev, world, ms_fp64=None) -
         out.append({"precision": prec, "format": fmt[prec], "value": value, "unit": UNIT,
                     "ms_per_step": 1e3 * elapsed / args.steps, "ms_per_sweep_kernel": ms_sweep,
                     "dtype": "fp16/bf16 split products, fp32 accumulate and faces, f64 vo",
-                    "gpu_launches": 2 * args.steps * NITER, "clocks": clk,
-                    "launches_per_sweep": "2: the sweep kernel and the FP64 sum of the eight octant partials",
+                    "gpu_launches": 3 * args.steps * NITER, "clocks": clk,
+                    "launches_per_sweep": "3: vi converted to FP16/BF16 hi+lo operand blocks, the sweep kernel, "
+                                          "and the FP64 sum of the eight octant partials",
                     "step": "%d sweeps of the initial state (not fed back: see error_note)" % NITER,
                     "error_builtin": {"max_rel": one_max, "normsq_rel": one_nsq},
                     "error_note": "errors of one sweep against the FP64 sweep of the same input; fed back, "
@@ -385,7 +386,7 @@ def measure_dense(args, dev, world: int, local_rank: int) -> dict | None:
             torch.cuda.synchronize()
             ms = max_over_ranks(e0.elapsed_time(e1) / 1e3) * 1e3
             r = {"precision": prec, "ms_per_sweep": ms, "updates_per_s": upd * world / (ms * 1e-3),
-                 "launches_per_sweep": (na + 63) // 64 if prec == 0 else 2 * ((na + 31) // 32)}
+                 "launches_per_sweep": (na + 63) // 64 if prec == 0 else 1 + 2 * ((na + 31) // 32)}
             if prec == 0:
                 r["exact"] = bool(torch.equal(va, vb))
                 r["tflops"] = flops / (ms * 1e-3) / 1e12
@@ -550,7 +551,7 @@ def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict |
                                "definition": "completion time of each problem counted from the start of the "
                                              "sequence (rank 0's share)"},
                 "error_vs_fp64_max_over_problems": {"max_rel": mix_rel, "normsq_rel": mix_nsq},
-                "launches_per_problem": "2 per 32-angle pass (sweep kernel + partial sum)",
+                "launches_per_problem": "1 (vi conversion) + 2 per 32-angle pass (sweep kernel + partial sum)",
                 "note": "one mixed-precision Sweeper per problem, swept one after another: the persistent "
                         "batched kernel sweeps in FP64 only"},
             "problems_per_rank": len(probs), "ntask": info["ntask"],

@@ -588,7 +588,8 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
                        "status copy")))
     return rc;
   const int npass = (S.dims.na + pass_angles(S) - 1) / pass_angles(S);
-  S.nlaunch = (S.var.mix ? 2 : 1) * npass;
+  // mixed: the vi conversion, then the sweep kernel and the partial sum per pass
+  S.nlaunch = S.var.mix ? 1 + 2 * npass : npass;
   return MSB_OK;
 }
 
