@@ -747,6 +747,9 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> int:
     return finish({"value": updates_per_sweep() * NITER * e2e_steps * world / e2e_s, "unit": UNIT,
                    "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                    "path": "Sweeper_sweep_iterations (host vi in, 10 device sweeps, host result out)",
+                   "group_slices": pb.iterations_slices(),
+                   "overlap": "the groups are swept in slices of group pairs, each through all 10 sweeps; a "
+                              "slice's host copies overlap the other slices' sweeps (same results)",
                    "result_matches": e2e_ok})
 
 

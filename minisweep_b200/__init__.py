@@ -134,6 +134,7 @@ def lib() -> ctypes.CDLL:
                                                P(Quantities), P(Env)]
         L.msb_measure_fp64_peak.argtypes = [P(D), P(D), ctypes.c_int]
         L.Sweeper_last_stats.argtypes = [P(Sweeper), P(ctypes.c_longlong), P(ctypes.c_int)]
+        L.msb_iterations_slices.argtypes = [P(Sweeper)]
         L.Sweeper_debug_tasks.argtypes = [P(Sweeper), P(ctypes.c_int), ctypes.c_longlong]
         L.Sweeper_debug_tasks.restype = ctypes.c_longlong
         L.Sweeper_set_spin_limit.argtypes = [P(Sweeper), ctypes.c_longlong]
@@ -386,6 +387,13 @@ class Problem:
         _check(lib().Sweeper_sweep_iterations(ctypes.byref(self.sweeper), ctypes.c_void_p(out_ptr),
                                               ctypes.c_void_p(in_ptr), niterations, ctypes.byref(self.quan),
                                               ctypes.byref(self.env)))
+
+    def iterations_slices(self) -> int:
+        """Group-pair slices the last sweep_iterations_host call ran in (1: whole)."""
+        r = lib().msb_iterations_slices(ctypes.byref(self.sweeper))
+        if r < 0:
+            _check(r)
+        return r
 
     def sync(self) -> None:
         _check(lib().Sweeper_sync_status(ctypes.byref(self.sweeper), ctypes.byref(self.env)))

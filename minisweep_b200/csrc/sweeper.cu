@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <memory>
 #include <new>
@@ -200,6 +201,19 @@ struct KbaState {
   }
 };
 
+// Task tables of a run split into slices of group pairs (see
+// sweep_iterations_sliced): slice k holds the plan's tasks of group pairs
+// [gp0[k], gp0[k + 1]) in the plan's order, dependencies renumbered.
+struct SliceTables {
+  const int* for_tasks = nullptr;  // the plan's table they were cut from
+  std::vector<int> gp0;
+  std::vector<int*> d_tasks;
+  std::vector<long long> ntask;
+  ~SliceTables() {
+    for (int* p : d_tasks) cudaFree(p);
+  }
+};
+
 struct SweeperImpl {
   Dimensions dims{};
   int precision = 0;
@@ -237,6 +251,8 @@ struct SweeperImpl {
   int l2_hints = 0;               // --l2_hints: L2 eviction policies in the chained FP64 kernel
   int sp_off = 0;                 // (ix_base + 3 iy_base) & 3 of a decomposed process's subdomain
   std::unique_ptr<KbaState> kba;  // set: the sweep is decomposed over a process grid
+  std::unique_ptr<SliceTables> slices;  // Sweeper_sweep_iterations in group-pair slices
+  int run_slices = 0;                   // slices of the last Sweeper_sweep_iterations (1: whole)
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
@@ -601,6 +617,156 @@ static int impl_sync(SweeperImpl& S, cudaStream_t stream) {
     return set_error(MSB_ERR_TIMEOUT, "a device wait ran out of time (task %d); sweep aborted", S.h_status[SY_ERRTASK]);
   if (err) return set_error(err, "device error %d", err);
   return MSB_OK;
+}
+
+// ------------------------------------------- host-buffer runs in group slices
+// The energy groups are independent in the sweep (no face, dependency or sum
+// crosses them), so a run of Sweeper_sweep_iterations on a large FP64 problem
+// is split into slices of group pairs, each swept through every iteration
+// with its own task table: the host->device copy of slice k + 1 then runs
+// while slice k is swept, and the device->host copy of slice k while slice
+// k + 1 is.  Every value is the one the unsliced run computes.  Slices are
+// used only where they stay efficient (64^3 cells x na 32, one B200: 115.9 ms
+// per sweep with 64 groups, 58.2 with 32, 29.8 with 16, 16.4 with 8).
+static int slice_count(const SweeperImpl& S) {
+  if (S.kba || !S.var.fn || (S.autotune && !S.tuned)) return 1;
+  const size_t bytes = Dimensions_size_state(S.dims, NU) * sizeof(double);
+  if (bytes < ((size_t)256 << 20)) return 1;  // copies too short to be worth hiding
+  return std::max(1, std::min(4, S.ngp / 8));
+}
+
+static int build_slices(SweeperImpl& S, int nslice) {
+  if (S.slices && S.slices->for_tasks == S.d_tasks && (int)S.slices->d_tasks.size() == nslice) return MSB_OK;
+  S.slices.reset();
+  auto T = std::make_unique<SliceTables>();
+  T->for_tasks = S.d_tasks;
+  const long long n = S.sched.ntask();
+  const int* rec = S.sched.rec.data();
+  std::vector<long long> index(n, -1);  // task -> its index in its slice
+  for (int k = 0; k <= nslice; ++k) T->gp0.push_back((int)((long long)S.ngp * k / nslice));
+  for (int k = 0; k < nslice; ++k) {
+    const int g0 = T->gp0[k], g1 = T->gp0[k + 1];
+    std::vector<int> out;
+    long long m = 0;
+    for (long long t = 0; t < n; ++t) {
+      const int* r = rec + (size_t)t * MSB_TASK_INTS;
+      if (r[TK_GP] < g0 || r[TK_GP] >= g1) continue;
+      index[t] = m++;
+      out.insert(out.end(), r, r + MSB_TASK_INTS);
+      int* q = out.data() + out.size() - MSB_TASK_INTS;
+      for (int f : {TK_DEP_X, TK_DEP_Y, TK_DEP_Z, TK_DEP_VO}) {
+        if (q[f] < 0) continue;
+        const int gd = rec[(size_t)q[f] * MSB_TASK_INTS + TK_GP];
+        if (q[f] >= t || gd < g0 || gd >= g1)
+          return set_error(MSB_ERR_ARG, "schedule: task %lld depends on task %d outside its slice", t, q[f]);
+        q[f] = (int)index[q[f]];
+      }
+    }
+    int* d = nullptr;
+    int rc = cuda_check(cudaMalloc(&d, std::max<size_t>(out.size(), 1) * sizeof(int)), "cudaMalloc slice tasks");
+    if (rc) return rc;
+    T->d_tasks.push_back(d);
+    if ((rc = cuda_check(cudaMemcpy(d, out.data(), out.size() * sizeof(int), cudaMemcpyHostToDevice),
+                         "upload slice tasks")))
+      return rc;
+    T->ntask.push_back(m);
+  }
+  S.slices = std::move(T);
+  return MSB_OK;
+}
+
+// Groups [e0, e1) of a state array: one contiguous run per z-plane.
+static int copy_groups(double* dst, const double* src, const Dimensions& d, int e0, int e1, cudaMemcpyKind kind,
+                       cudaStream_t st) {
+  const size_t slab = (size_t)d.nm * NU * d.ncell_x * d.ncell_y;
+  const size_t pitch = (size_t)d.ne * slab * sizeof(double), width = (size_t)(e1 - e0) * slab * sizeof(double);
+  const size_t off = (size_t)e0 * slab;
+  if (width == pitch) return cuda_check(cudaMemcpyAsync(dst, src, pitch * d.ncell_z, kind, st), "state copy");
+  if (pitch <= (size_t)INT_MAX)
+    return cuda_check(cudaMemcpy2DAsync(dst + off, pitch, src + off, pitch, width, d.ncell_z, kind, st),
+                      "state copy");
+  for (int iz = 0; iz < d.ncell_z; ++iz) {
+    const size_t o = off + (size_t)iz * d.ne * slab;
+    int rc = cuda_check(cudaMemcpyAsync(dst + o, src + o, width, kind, st), "state copy");
+    if (rc) return rc;
+  }
+  return MSB_OK;
+}
+
+// in_h -> (niterations sweeps) -> out_h in nslice group slices on three
+// streams: copies in (sh), the sweeps (st, the Env's stream), copies out
+// (sd).  The task counter and progress words start over before every sweep
+// but the error words do not, so a failed sweep makes the later ones end at
+// once and the final status reports it.
+static int sweep_iterations_sliced(SweeperImpl& S, int nslice, double* out_h, const double* in_h, int niterations,
+                                   const double* afm_h, const double* mfa_h, const double* afm_d,
+                                   const double* mfa_d, cudaStream_t st) {
+  int rc = build_slices(S, nslice);
+  if (rc) return rc;
+  const SliceTables& T = *S.slices;
+  const Dimensions& d = S.dims;
+  cudaStream_t sh = nullptr, sd = nullptr;
+  std::vector<cudaEvent_t> ev(2 * nslice + 2, nullptr);  // [0] start, [1 + k] slice k in, [1 + nslice + k] swept, end
+  bool enqueued = false;
+  rc = cuda_check(cudaStreamCreateWithFlags(&sh, cudaStreamNonBlocking), "copy stream");
+  if (!rc) rc = cuda_check(cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking), "copy stream");
+  for (auto& e : ev)
+    if (!rc) rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "slice event");
+  // the copies wait for the work already on the Env's stream
+  if (!rc) rc = cuda_check(cudaEventRecord(ev[0], st), "slice event");
+  if (!rc) rc = cuda_check(cudaStreamWaitEvent(sh, ev[0], 0), "slice wait");
+  if (!rc) rc = cuda_check(cudaStreamWaitEvent(sd, ev[0], 0), "slice wait");
+  if (!rc) rc = load_matrices(S, afm_h, mfa_h, afm_d, mfa_d, st);
+  if (!rc) rc = cuda_check(cudaMemsetAsync(S.d_sync, 0, S.sync_ints * sizeof(int), st), "reset sync");
+  auto groups = [&](int k, int& e0, int& e1) {
+    e0 = 2 * T.gp0[k];
+    e1 = std::min(2 * T.gp0[k + 1], d.ne);
+  };
+  for (int k = 0; k < nslice && !rc; ++k) {
+    int e0, e1;
+    groups(k, e0, e1);
+    enqueued = true;
+    rc = copy_groups(S.d_vi, in_h, d, e0, e1, cudaMemcpyHostToDevice, sh);
+    if (!rc) rc = cuda_check(cudaEventRecord(ev[1 + k], sh), "slice event");
+  }
+  double* last = (niterations % 2) ? S.d_vo : S.d_vi;  // where the last sweep writes
+  for (int k = 0; k < nslice && !rc; ++k) {
+    rc = cuda_check(cudaStreamWaitEvent(st, ev[1 + k], 0), "slice wait");
+    double* a = S.d_vi;
+    double* b = S.d_vo;
+    for (int it = 0; it < niterations && !rc; ++it) {
+      if (k > 0 || it > 0) rc = reset_pass(S, st);
+      if (!rc) rc = launch_fp64(S, S.var, T.d_tasks[k], T.ntask[k], S.grid, b, a, st);
+      std::swap(a, b);
+    }
+    int e0, e1;
+    groups(k, e0, e1);
+    if (!rc) rc = cuda_check(cudaEventRecord(ev[1 + nslice + k], st), "slice event");
+    if (!rc) rc = cuda_check(cudaStreamWaitEvent(sd, ev[1 + nslice + k], 0), "slice wait");
+    if (!rc) rc = copy_groups(out_h, last, d, e0, e1, cudaMemcpyDeviceToHost, sd);
+  }
+  // the Env's stream ends after the last copy out: its sync covers the run
+  if (!rc) rc = cuda_check(cudaEventRecord(ev.back(), sd), "slice event");
+  if (!rc) rc = cuda_check(cudaStreamWaitEvent(st, ev.back(), 0), "slice wait");
+  if (!rc)
+    rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, st),
+                    "status copy");
+  if (!rc) rc = impl_sync(S, st);
+  if (rc && enqueued) {
+    // nothing may still write the caller's buffer after the error is returned
+    cudaStreamSynchronize(sh);
+    cudaStreamSynchronize(st);
+    cudaStreamSynchronize(sd);
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (sh) cudaStreamDestroy(sh);
+  if (sd) cudaStreamDestroy(sd);
+  if (!rc) {
+    const int npass = (d.na + pass_angles(S) - 1) / pass_angles(S);
+    S.nlaunch = npass;
+  }
+  return rc;
 }
 
 // ------------------------------------------------------- KBA decomposition
@@ -1111,6 +1277,12 @@ extern "C" long long Sweeper_debug_tasks(const Sweeper* sweeper, int* out, long 
   return n;
 }
 
+extern "C" int msb_iterations_slices(const Sweeper* sweeper) {
+  const SweeperImpl* S = impl_of(sweeper);
+  if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
+  return S->run_slices;
+}
+
 extern "C" int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit) {
   SweeperImpl* S = impl_of(sweeper);
   if (!S) return msb::set_error(MSB_ERR_ARG, "Sweeper not created");
@@ -1121,7 +1293,9 @@ extern "C" int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit) {
 // A whole run of the reference driver's iteration loop (runner.c:148-155) on
 // the device: v_in_h (host) is copied in once, niterations sweeps ping-pong
 // between two device arrays (the vi/vo swap), and the last sweep's output is
-// copied to v_out_h.  Pinned host buffers make the copies asynchronous.
+// copied to v_out_h.  Pinned host buffers make the copies asynchronous; on a
+// large FP64 problem the run goes in group-pair slices whose copies overlap
+// the other slices' sweeps (sweep_iterations_sliced).
 extern "C" int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const double* v_in_h, int niterations,
                                         const Quantities* quan, Env* env) {
   SweeperImpl* S = impl_of(sweeper);
@@ -1132,6 +1306,14 @@ extern "C" int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const
   int rc;
   if (!S->d_vi && (rc = msb::cuda_check(cudaMalloc(&S->d_vi, n * sizeof(double)), "cudaMalloc vi"))) return rc;
   if (!S->d_vo && (rc = msb::cuda_check(cudaMalloc(&S->d_vo, n * sizeof(double)), "cudaMalloc vo"))) return rc;
+  const int nslice = niterations > 0 && quan ? msb::slice_count(*S) : 1;
+  S->run_slices = nslice;
+  if (nslice > 1) {
+    const bool mats_on_dev = quan->a_from_m.d_ && quan->m_from_a.d_;
+    return msb::sweep_iterations_sliced(*S, nslice, v_out_h, v_in_h, niterations, quan->a_from_m.h_,
+                                        quan->m_from_a.h_, mats_on_dev ? quan->a_from_m.d_ : nullptr,
+                                        mats_on_dev ? quan->m_from_a.d_ : nullptr, st);
+  }
   if ((rc = msb::cuda_check(cudaMemcpyAsync(S->d_vi, v_in_h, n * sizeof(double), cudaMemcpyHostToDevice, st), "H2D")))
     return rc;
   double* a = S->d_vi;
