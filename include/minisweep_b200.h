@@ -334,12 +334,12 @@ int Sweeper_sync_status(Sweeper* sweeper, Env* env);
  * (host).  Synchronous; returns the status of the device work. */
 int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const double* v_in_h, int niterations,
                              const Quantities* quan, Env* env);
-/* Group-pair slices the last Sweeper_sweep_iterations call ran in (1: the
- * whole problem at once; 0: no call yet).  On a large FP64 problem (state of
- * 256 MiB or more, 16 or more group pairs) the groups are swept in up to 4
- * slices, each through every iteration, so that a slice's host copies overlap
- * the other slices' sweeps; the results are the same.  No reference
- * counterpart. */
+/* Group-pair slices the last host-buffer call (Sweeper_sweep[_status] or
+ * Sweeper_sweep_iterations) ran in (1: the whole problem at once; 0: no call
+ * yet).  On a large FP64 problem (state of 256 MiB or more, 16 or more group
+ * pairs) those calls sweep the groups in up to 4 slices, each through every
+ * iteration, so that a slice's host copies overlap the other slices' sweeps;
+ * the results are the same.  No reference counterpart. */
 int msb_iterations_slices(const Sweeper* sweeper);
 /* Device-side FP64 checksums of two device state arrays (same sums as
  * get_state_norms). */

@@ -389,7 +389,7 @@ class Problem:
                                               ctypes.byref(self.env)))
 
     def iterations_slices(self) -> int:
-        """Group-pair slices the last sweep_iterations_host call ran in (1: whole)."""
+        """Group-pair slices the last sweep_host / sweep_iterations_host call ran in (1: whole)."""
         r = lib().msb_iterations_slices(ctypes.byref(self.sweeper))
         if r < 0:
             _check(r)

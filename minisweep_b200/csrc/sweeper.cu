@@ -252,7 +252,7 @@ struct SweeperImpl {
   int sp_off = 0;                 // (ix_base + 3 iy_base) & 3 of a decomposed process's subdomain
   std::unique_ptr<KbaState> kba;  // set: the sweep is decomposed over a process grid
   std::unique_ptr<SliceTables> slices;  // Sweeper_sweep_iterations in group-pair slices
-  int run_slices = 0;                   // slices of the last Sweeper_sweep_iterations (1: whole)
+  int run_slices = 0;                   // slices of the last host-buffer sweep call (1: whole)
 
   ~SweeperImpl() {
     cudaFree(d_tasks);
@@ -695,12 +695,13 @@ static int copy_groups(double* dst, const double* src, const Dimensions& d, int 
 
 // in_h -> (niterations sweeps) -> out_h in nslice group slices on three
 // streams: copies in (sh), the sweeps (st, the Env's stream), copies out
-// (sd).  The task counter and progress words start over before every sweep
+// (sd).  in_h lands in the device array d_a; the sweeps alternate between
+// d_a and d_b (the vi/vo swap).  The task counter and progress words start over before every sweep
 // but the error words do not, so a failed sweep makes the later ones end at
 // once and the final status reports it.
 static int sweep_iterations_sliced(SweeperImpl& S, int nslice, double* out_h, const double* in_h, int niterations,
-                                   const double* afm_h, const double* mfa_h, const double* afm_d,
-                                   const double* mfa_d, cudaStream_t st) {
+                                   double* d_a, double* d_b, const double* afm_h, const double* mfa_h,
+                                   const double* afm_d, const double* mfa_d, cudaStream_t st) {
   int rc = build_slices(S, nslice);
   if (rc) return rc;
   const SliceTables& T = *S.slices;
@@ -722,29 +723,40 @@ static int sweep_iterations_sliced(SweeperImpl& S, int nslice, double* out_h, co
     e0 = 2 * T.gp0[k];
     e1 = std::min(2 * T.gp0[k + 1], d.ne);
   };
-  for (int k = 0; k < nslice && !rc; ++k) {
+  // Host order: copy in k + 1 and copy out k - 1 are issued after slice k's
+  // sweeps, so that with pageable host buffers (whose copies return only
+  // once done) the GPU is sweeping while the host thread copies.
+  auto copy_in = [&](int k) {
     int e0, e1;
     groups(k, e0, e1);
     enqueued = true;
-    rc = copy_groups(S.d_vi, in_h, d, e0, e1, cudaMemcpyHostToDevice, sh);
-    if (!rc) rc = cuda_check(cudaEventRecord(ev[1 + k], sh), "slice event");
-  }
-  double* last = (niterations % 2) ? S.d_vo : S.d_vi;  // where the last sweep writes
+    int r = copy_groups(d_a, in_h, d, e0, e1, cudaMemcpyHostToDevice, sh);
+    if (!r) r = cuda_check(cudaEventRecord(ev[1 + k], sh), "slice event");
+    return r;
+  };
+  double* last = (niterations % 2) ? d_b : d_a;  // where the last sweep writes
+  auto copy_out = [&](int k) {
+    int e0, e1;
+    groups(k, e0, e1);
+    int r = cuda_check(cudaStreamWaitEvent(sd, ev[1 + nslice + k], 0), "slice wait");
+    if (!r) r = copy_groups(out_h, last, d, e0, e1, cudaMemcpyDeviceToHost, sd);
+    return r;
+  };
+  if (!rc) rc = copy_in(0);
   for (int k = 0; k < nslice && !rc; ++k) {
     rc = cuda_check(cudaStreamWaitEvent(st, ev[1 + k], 0), "slice wait");
-    double* a = S.d_vi;
-    double* b = S.d_vo;
+    double* a = d_a;
+    double* b = d_b;
     for (int it = 0; it < niterations && !rc; ++it) {
       if (k > 0 || it > 0) rc = reset_pass(S, st);
       if (!rc) rc = launch_fp64(S, S.var, T.d_tasks[k], T.ntask[k], S.grid, b, a, st);
       std::swap(a, b);
     }
-    int e0, e1;
-    groups(k, e0, e1);
     if (!rc) rc = cuda_check(cudaEventRecord(ev[1 + nslice + k], st), "slice event");
-    if (!rc) rc = cuda_check(cudaStreamWaitEvent(sd, ev[1 + nslice + k], 0), "slice wait");
-    if (!rc) rc = copy_groups(out_h, last, d, e0, e1, cudaMemcpyDeviceToHost, sd);
+    if (!rc && k + 1 < nslice) rc = copy_in(k + 1);
+    if (!rc && k > 0) rc = copy_out(k - 1);
   }
+  if (!rc) rc = copy_out(nslice - 1);
   // the Env's stream ends after the last copy out: its sync covers the run
   if (!rc) rc = cuda_check(cudaEventRecord(ev.back(), sd), "slice event");
   if (!rc) rc = cuda_check(cudaStreamWaitEvent(st, ev.back(), 0), "slice wait");
@@ -1224,6 +1236,15 @@ extern "C" int Sweeper_sweep_status(Sweeper* sweeper, Pointer* vo, Pointer* vi, 
     if (!vi_d) vi_d = S->d_vi;
     if (!vo_d) vo_d = S->d_vo;
   }
+  // a large FP64 problem: the copies overlap the sweep, slice by slice
+  const int nslice = quan && vi_d != vo_d ? msb::slice_count(*S) : 1;
+  S->run_slices = nslice;
+  if (nslice > 1) {
+    const bool mats_on_dev = quan->a_from_m.d_ && quan->m_from_a.d_;
+    return msb::sweep_iterations_sliced(*S, nslice, vo->h_, vi->h_, 1, vi_d, vo_d, quan->a_from_m.h_,
+                                        quan->m_from_a.h_, mats_on_dev ? quan->a_from_m.d_ : nullptr,
+                                        mats_on_dev ? quan->m_from_a.d_ : nullptr, st);
+  }
   if ((rc = msb::cuda_check(cudaMemcpyAsync(vi_d, vi->h_, n * sizeof(double), cudaMemcpyHostToDevice, st), "vi H2D")))
     return rc;
   if ((rc = Sweeper_sweep_device(sweeper, vo_d, vi_d, quan, env))) return rc;
@@ -1310,8 +1331,9 @@ extern "C" int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const
   S->run_slices = nslice;
   if (nslice > 1) {
     const bool mats_on_dev = quan->a_from_m.d_ && quan->m_from_a.d_;
-    return msb::sweep_iterations_sliced(*S, nslice, v_out_h, v_in_h, niterations, quan->a_from_m.h_,
-                                        quan->m_from_a.h_, mats_on_dev ? quan->a_from_m.d_ : nullptr,
+    return msb::sweep_iterations_sliced(*S, nslice, v_out_h, v_in_h, niterations, S->d_vi, S->d_vo,
+                                        quan->a_from_m.h_, quan->m_from_a.h_,
+                                        mats_on_dev ? quan->a_from_m.d_ : nullptr,
                                         mats_on_dev ? quan->m_from_a.d_ : nullptr, st);
   }
   if ((rc = msb::cuda_check(cudaMemcpyAsync(S->d_vi, v_in_h, n * sizeof(double), cudaMemcpyHostToDevice, st), "H2D")))

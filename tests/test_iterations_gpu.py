@@ -66,6 +66,17 @@ def test_iterations_match_device_sweeps(nx, ny, nz, ne, na, nm, niter, slices):
     assert np.array_equal(got, ref), f"max abs diff {np.max(np.abs(got - ref))}"
 
 
+def test_host_pointer_sweep_sliced():
+    """Sweeper_sweep (host Pointers, the reference driver's call) goes in
+    slices too."""
+    with msb.Problem(flags(32, 32, 32, 32, 32), nm=16) as pb:
+        vi = random_state(pb, 4)
+        ref = device_iterations(pb, vi, 1)
+        got = pb.sweep_host(vi)
+        assert pb.iterations_slices() == 2
+    assert np.array_equal(got, ref)
+
+
 def test_sliced_run_from_pageable_buffers():
     with msb.Problem(flags(32, 32, 32, 32, 32), nm=16) as pb:
         vi = random_state(pb, 9)
