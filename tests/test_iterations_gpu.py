@@ -105,3 +105,20 @@ def test_zero_iterations_copy_through():
         got = host_iterations(pb, vi, 0)
         assert pb.iterations_slices() == 1
     assert np.array_equal(got, vi)
+
+
+def test_sliced_run_reports_timeout_and_recovers():
+    """A forced 1 ns wait budget: the first wait that spins gives up, the
+    error survives the later slices' sweeps (which end at once) and the call
+    returns MSB_ERR_TIMEOUT; with the default budget the next call is right."""
+    with msb.Problem(flags(32, 32, 32, 32, 32), nm=16) as pb:
+        vi = random_state(pb, 6)
+        ref = device_iterations(pb, vi, 2)
+        pb.set_timeout_ns(1)
+        with pytest.raises(msb.SweepError) as e:
+            host_iterations(pb, vi, 2)
+        assert e.value.code == msb.MSB_ERR_TIMEOUT
+        assert pb.iterations_slices() == 2
+        pb.set_timeout_ns(0)
+        got = host_iterations(pb, vi, 2)
+    assert np.array_equal(got, ref)
