@@ -560,10 +560,84 @@ def measure_batched(args, dev, world: int, rank: int, local_rank: int) -> dict |
             "scratch_gb": info["scratch_bytes"] / 1e9, "scratch_needed_all_gb": info["scratch_needed_all"] / 1e9,
             "scratch_waits": info["npred"], "create_s": create_s, "autotune_ms": info["tune_ms"],
             "sm_utilisation_simulated": sim,
+            "small_problems": measure_small_batch(dev, world, rank),
             "clocks": clk,
             "note": "one persistent launch sweeps every problem; the face scratch of all problems at once "
                     "does not fit beside the state, so problems reuse the scratch of completed ones (device-side "
                     "waits on per-problem completion counters)"}
+
+
+def measure_small_batch(dev, world: int, rank: int) -> dict:
+    """Many small problems (msb.small_batch_workload: 256 problems from seed
+    11, 4..12 cells a side, 2..8 groups), the serving case batching is for:
+    one persistent launch per sweep against the same problems swept one
+    Sweeper (one launch) after another, each after one untimed sweep."""
+    import numpy as np
+    import torch
+
+    import minisweep_b200 as msb
+    from minisweep_b200.parallel import max_over_ranks
+
+    W = msb.small_batch_workload()
+    probs = [W[i] for i in range(len(W)) if i % world == rank]
+    vis, vos, mats, descs = [], [], {}, []
+    for q in probs:
+        vi = torch.empty(msb.state_size(q), dtype=torch.float64, device=dev)
+        msb.init_state_device(vi.data_ptr(), q)
+        key = (q["nm"], q["na"])
+        if key not in mats:
+            a, m = msb.builtin_matrices(*key)
+            mats[key] = (torch.from_numpy(a).to(dev), torch.from_numpy(m).to(dev))
+        vis.append(vi)
+        vos.append(torch.empty_like(vi))
+        descs.append(dict(q, vi=vi.data_ptr(), vo=vos[-1].data_ptr(), a_from_m=mats[key][0].data_ptr(),
+                          m_from_a=mats[key][1].data_ptr()))
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream(device=dev)
+    sh = s.cuda_stream
+    with msb.Batch(descs, autotune=True) as b:
+        def timed(fn):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            b.sync(sh)
+            return e0.elapsed_time(e1)
+
+        for _ in range(2):
+            b.sweep(0, sh)
+            b.sync(sh)
+        batch_ms = min(timed(lambda: b.sweep(0, sh)) for _ in range(3))
+        done_ms = b.problem_ms()
+    seq_ms, exact = 0.0, True
+    for i, q in enumerate(probs):
+        fl = f"--ncell_x {q['ncell_x']} --ncell_y {q['ncell_y']} --ncell_z {q['ncell_z']} --ne {q['ne']} --na {q['na']}"
+        with msb.Problem(fl, nm=q["nm"]) as pb1:
+            out = torch.empty_like(vis[i])
+            st1 = torch.cuda.ExternalStream(pb1.stream) if pb1.stream else torch.cuda.current_stream()
+            pb1.sweep_device(out.data_ptr(), vis[i].data_ptr())
+            pb1.sync()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st1)
+            pb1.sweep_device(out.data_ptr(), vis[i].data_ptr())
+            e1.record(st1)
+            pb1.sync()
+            seq_ms += e0.elapsed_time(e1)
+            exact = exact and bool(torch.equal(out, vos[i]))
+    batch_ms = max_over_ranks(batch_ms / 1e3) * 1e3
+    seq_ms = max_over_ranks(seq_ms / 1e3) * 1e3
+    del vis, vos, descs, mats
+    torch.cuda.empty_cache()
+    return {"workload": "256 small problems from seed 11 (numpy PCG64): ncell_x,y in {4..12}, ncell_z in "
+                        "{4..16}, ne in {2,4,8}, na in {16,32}, NM in {4,16}, NU 4, built-in Quantities, FP64",
+            "value": len(W) / (batch_ms / 1e3), "unit": "problems/s", "ms_per_batch_sweep": batch_ms,
+            "unbatched_ms": seq_ms, "speedup_vs_unbatched": seq_ms / batch_ms, "exact_vs_sweeper": exact,
+            "latency_ms": {"p50": float(np.percentile(done_ms, 50)), "p99": float(np.percentile(done_ms, 99))},
+            "note": "each of these problems alone leaves most SMs idle; one launch sweeps them all side by "
+                    "side (unbatched: one Sweeper per problem, default plan, timed after one untimed sweep)"}
 
 
 def run_ours(args, rank: int, world: int, local_rank: int) -> int:

@@ -539,6 +539,21 @@ def batch_workload(n: int = 256, seed: int = 7) -> list:
                  nm=int(nm[i])) for i in range(n)]
 
 
+def small_batch_workload(n: int = 256, seed: int = 11) -> list:
+    """Many small problems, the case batching is for (each alone leaves most
+    SMs idle): drawn with numpy's PCG64 from `seed`, per problem in this
+    order: ncell_x, ncell_y uniform in {4..12}, ncell_z in {4..16}, ne from
+    {2, 4, 8}, na from {16, 32}, nm from {4, 16} (NU = 4, built-in
+    Quantities)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n):
+        nx, ny, nz = int(rng.integers(4, 13)), int(rng.integers(4, 13)), int(rng.integers(4, 17))
+        ne, na, nm = int(rng.choice([2, 4, 8])), int(rng.choice([16, 32])), int(rng.choice([4, 16]))
+        out.append(dict(ncell_x=nx, ncell_y=ny, ncell_z=nz, ne=ne, na=na, nm=nm))
+    return out
+
+
 def state_size(p: dict) -> int:
     return p["ncell_x"] * p["ncell_y"] * p["ncell_z"] * p["ne"] * p["nm"] * NU
 

@@ -81,6 +81,18 @@ def test_batch_matches_single_sweepers():
         assert np.array_equal(got, ref), (i, p)
 
 
+def test_batch_small_problem_workload():
+    """The first 48 problems of the small-problem serving workload (many
+    problems that each leave most SMs idle), against their own Sweepers."""
+    W = msb.small_batch_workload()[:48]
+    D = Device(W)
+    with msb.Batch(D.descs, autotune=True) as b:
+        b.sweep(0)
+        b.sync()
+    for i, p in enumerate(W):
+        assert np.array_equal(D.vo[i].cpu().numpy(), single(p, D.host_vi[i])), (i, p)
+
+
 def test_batch_matches_oracle():
     probs = PROBLEMS[:3]
     D = Device(probs)
