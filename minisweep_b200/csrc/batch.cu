@@ -259,34 +259,46 @@ int simulate_and_order(BatchImpl& B) {
   for (int p = 0; p < np; ++p) first[p + 1] = first[p] + B.probs[p].sched.ntask();
   const long long N = first[np];
   if (N >= (1LL << 31) - SY_PROGRESS - np - 1) return set_error(MSB_ERR_ARG, "batch: too many tasks (%lld)", N);
-  std::vector<int> tprob(N);
-  std::vector<float> dur(N), plane_delay(N);
-  std::vector<int> left(N);
-  // dependents: CSR, value = dependent id * 2 + (1 if released by the plane event)
-  std::vector<int> dcount(N + 1, 0);
+  // per task, in one record (the simulation touches them together): its
+  // problem, duration, delay until its first plane is through, and the
+  // dependencies not yet released
+  struct SimTask {
+    float dur, plane_delay;
+    int left, prob;
+  };
+  std::vector<SimTask> T(N);
+  // dependents, CSR: dcount/dlist released when a task completes, pcount/plist
+  // when its first plane is through (a same-phase neighbour's plane-by-plane
+  // dependency)
+  std::vector<int> dcount(N + 1, 0), pcount(N + 1, 0);
   for (int p = 0; p < np; ++p) {
     const ProbPlan& P = B.probs[p];
     const double c = step_cost(P.d.nm, P.nch);
     for (long long t = 0; t < P.sched.ntask(); ++t) {
       const int* r = &P.sched.rec[t * MSB_TASK_INTS];
       const long long g = first[p] + t;
-      tprob[g] = p;
+      T[g].prob = p;
       const int w = r[TK_X1] - r[TK_X0], h = r[TK_Y1] - r[TK_Y0], nz = r[TK_Z1] - r[TK_Z0];
-      dur[g] = (float)(c * (nz + w + h - 2));
-      plane_delay[g] = (float)(c * (w + h - 1));
+      T[g].dur = (float)(c * (nz + w + h - 2));
+      T[g].plane_delay = (float)(c * (w + h - 1));
       int n = 0;
       for (int k = TK_DEP_X; k <= TK_DEP_VO; ++k)
         if (r[k] >= 0) {
           ++n;
-          ++dcount[first[p] + r[k] + 1];
+          const bool plane = (k == TK_DEP_X && (r[TK_DEP_MODE] & DM_X_PLANE)) ||
+                             (k == TK_DEP_Y && (r[TK_DEP_MODE] & DM_Y_PLANE));
+          ++(plane ? pcount : dcount)[first[p] + r[k] + 1];
         }
-      left[g] = n;
+      T[g].left = n;
     }
   }
-  for (long long g = 0; g < N; ++g) dcount[g + 1] += dcount[g];
-  std::vector<int> dlist(dcount[N]);
+  for (long long g = 0; g < N; ++g) {
+    dcount[g + 1] += dcount[g];
+    pcount[g + 1] += pcount[g];
+  }
+  std::vector<int> dlist(dcount[N]), plist(pcount[N]);
   {
-    std::vector<int> fill(dcount.begin(), dcount.end() - 1);
+    std::vector<int> fill(dcount.begin(), dcount.end() - 1), pfill(pcount.begin(), pcount.end() - 1);
     for (int p = 0; p < np; ++p) {
       const ProbPlan& P = B.probs[p];
       for (long long t = 0; t < P.sched.ntask(); ++t) {
@@ -296,7 +308,11 @@ int simulate_and_order(BatchImpl& B) {
           if (r[k] >= 0) {
             const bool plane = (k == TK_DEP_X && (r[TK_DEP_MODE] & DM_X_PLANE)) ||
                                (k == TK_DEP_Y && (r[TK_DEP_MODE] & DM_Y_PLANE));
-            dlist[fill[first[p] + r[k]]++] = (int)(g * 2 + (plane ? 1 : 0));
+            const long long u = first[p] + r[k];
+            if (plane)
+              plist[pfill[u]++] = (int)g;
+            else
+              dlist[fill[u]++] = (int)g;
           }
       }
     }
@@ -305,9 +321,36 @@ int simulate_and_order(BatchImpl& B) {
   const int ncls = (int)B.classes.size();
   std::vector<long long> cls_left(ncls, 0);
   for (int p = 0; p < np; ++p) cls_left[B.probs[p].cls] += B.probs[p].sched.ntask();
-  // ready tasks per class, by (admission order, index in the problem's schedule)
-  using RKey = std::pair<long long, long long>;  // (seq, g)
-  std::vector<std::priority_queue<RKey, std::vector<RKey>, std::greater<RKey>>> ready(ncls);
+  std::vector<int> by_seq(np);
+  for (int p = 0; p < np; ++p) by_seq[B.probs[p].seq] = p;
+  // ready tasks, taken by (admission order, index in the problem's
+  // schedule): a min-heap of task ids per problem, and per class a bit per
+  // admission slot whose problem has ready tasks
+  std::vector<std::priority_queue<long long, std::vector<long long>, std::greater<long long>>> ready(np);
+  const int nword = (np + 63) / 64;
+  std::vector<std::vector<uint64_t>> has_ready(ncls, std::vector<uint64_t>(nword, 0));
+  auto make_ready = [&](long long g) {
+    const int p = T[g].prob;
+    if (ready[p].empty()) {
+      const int q = B.probs[p].seq;
+      has_ready[B.probs[p].cls][q >> 6] |= 1ull << (q & 63);
+    }
+    ready[p].push(g);
+  };
+  // the next task of class c, or -1
+  auto take_ready = [&](int c) -> long long {
+    const std::vector<uint64_t>& w = has_ready[c];
+    for (int i = 0; i < nword; ++i)
+      if (w[i]) {
+        const int q = 64 * i + __builtin_ctzll(w[i]);
+        const int p = by_seq[q];
+        const long long g = ready[p].top();
+        ready[p].pop();
+        if (ready[p].empty()) has_ready[c][i] &= ~(1ull << (q & 63));
+        return g;
+      }
+    return -1;
+  };
   struct Ev {
     double t;
     int kind;  // 0 plane release, 1 finish
@@ -316,13 +359,11 @@ int simulate_and_order(BatchImpl& B) {
   };
   std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> ev;
   std::vector<long long> pdone(np, 0);
-  std::vector<int> by_seq(np);
-  for (int p = 0; p < np; ++p) by_seq[B.probs[p].seq] = p;
   Arena arena(B.arena_bytes);
   int next_admit = 0;
   auto push_ready = [&](int p) {
     for (long long t = first[p]; t < first[p + 1]; ++t)
-      if (left[t] == 0) ready[B.probs[p].cls].push({B.probs[p].seq, t});
+      if (T[t].left == 0) make_ready(t);
   };
   auto admit = [&]() {
     while (next_admit < np) {
@@ -344,12 +385,10 @@ int simulate_and_order(BatchImpl& B) {
     }
   };
   auto release = [&](long long g, bool plane) {
-    for (int k = dcount[g]; k < dcount[g + 1]; ++k) {
-      const int v = dlist[k];
-      if ((v & 1) != (plane ? 1 : 0)) continue;
-      const long long d = v >> 1;
-      if (--left[d] == 0) ready[B.probs[tprob[d]].cls].push({B.probs[tprob[d]].seq, d});
-    }
+    const std::vector<int>& cnt = plane ? pcount : dcount;
+    const std::vector<int>& lst = plane ? plist : dlist;
+    for (int k = cnt[g]; k < cnt[g + 1]; ++k)
+      if (--T[lst[k]].left == 0) make_ready(lst[k]);
   };
 
   std::vector<long long> table;
@@ -360,14 +399,14 @@ int simulate_and_order(BatchImpl& B) {
   admit();
   for (;;) {
     while (cur < ncls && cls_left[cur] == 0) ++cur;
-    while (free_w > 0 && cur < ncls && !ready[cur].empty()) {
-      const long long g = ready[cur].top().second;
-      ready[cur].pop();
+    while (free_w > 0 && cur < ncls) {
+      const long long g = take_ready(cur);
+      if (g < 0) break;
       table.push_back(g);
       --free_w;
       --cls_left[cur];
-      ev.push({now + dur[g], 1, g});
-      ev.push({now + plane_delay[g], 0, g});
+      ev.push({now + T[g].dur, 1, g});
+      ev.push({now + T[g].plane_delay, 0, g});
       while (cur < ncls && cls_left[cur] == 0) ++cur;
     }
     if (ev.empty()) break;
@@ -379,7 +418,7 @@ int simulate_and_order(BatchImpl& B) {
     } else {
       ++free_w;
       release(e.g, false);
-      const int p = tprob[e.g];
+      const int p = T[e.g].prob;
       if (++pdone[p] == B.probs[p].sched.ntask()) {
         const ProbPlan& P = B.probs[p];
         if (P.next >= 0) {
@@ -395,7 +434,7 @@ int simulate_and_order(BatchImpl& B) {
     return set_error(MSB_ERR_ARG, "batch: scheduling simulation left %lld tasks unplaced", N - (long long)table.size());
   B.sim_makespan = now;
   double busy = 0.0;
-  for (long long g = 0; g < N; ++g) busy += dur[g];
+  for (long long g = 0; g < N; ++g) busy += T[g].dur;
   B.sim_busy = now > 0.0 ? busy / (now * B.nsm) : 0.0;
 
   // the table in simulated start order, dependencies as global ids
@@ -405,18 +444,30 @@ int simulate_and_order(BatchImpl& B) {
   B.rec.assign((size_t)N * MSB_TASK_INTS, 0);
   B.task_prob.assign(N, 0);
   B.prob_ntask.assign(np, 0);
-  for (long long i = 0; i < N; ++i) {
-    const long long g = table[i];
-    const int p = tprob[g];
-    const int* r = &B.probs[p].sched.rec[(g - first[p]) * MSB_TASK_INTS];
-    int* o = &B.rec[i * MSB_TASK_INTS];
-    std::copy(r, r + MSB_TASK_INTS, o);
-    for (int k = TK_DEP_X; k <= TK_DEP_VO; ++k)
-      if (r[k] >= 0) {
-        o[k] = pos[first[p] + r[k]];
-        if (o[k] >= i) return set_error(MSB_ERR_ARG, "batch: table not topological");
-      }
-    B.task_prob[i] = p;
+  {
+    // independent records: written by the host's cores in chunks
+    std::atomic<bool> bad{false};
+    const int nthr = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&, t]() {
+        const long long i0 = N * t / nthr, i1 = N * (t + 1) / nthr;
+        for (long long i = i0; i < i1; ++i) {
+          const long long g = table[i];
+          const int p = T[g].prob;
+          const int* r = &B.probs[p].sched.rec[(g - first[p]) * MSB_TASK_INTS];
+          int* o = &B.rec[i * MSB_TASK_INTS];
+          std::copy(r, r + MSB_TASK_INTS, o);
+          for (int k = TK_DEP_X; k <= TK_DEP_VO; ++k)
+            if (r[k] >= 0) {
+              o[k] = pos[first[p] + r[k]];
+              if (o[k] >= i) bad = true;
+            }
+          B.task_prob[i] = p;
+        }
+      });
+    for (auto& th : pool) th.join();
+    if (bad) return set_error(MSB_ERR_ARG, "batch: table not topological");
   }
   for (int p = 0; p < np; ++p) B.prob_ntask[p] = (int)B.probs[p].sched.ntask();
   for (auto& c : B.classes) c.ntask = 0;
