@@ -355,7 +355,8 @@ int simulate_and_order(BatchImpl& B) {
     double t;
     int kind;  // 0 plane release, 1 finish
     long long g;
-    bool operator>(const Ev& o) const { return t != o.t ? t > o.t : kind > o.kind; }
+    // ties by kind, then task id: the order does not depend on the heap's layout
+    bool operator>(const Ev& o) const { return t != o.t ? t > o.t : kind != o.kind ? kind > o.kind : g > o.g; }
   };
   std::priority_queue<Ev, std::vector<Ev>, std::greater<Ev>> ev;
   std::vector<long long> pdone(np, 0);
@@ -406,7 +407,7 @@ int simulate_and_order(BatchImpl& B) {
       --free_w;
       --cls_left[cur];
       ev.push({now + T[g].dur, 1, g});
-      ev.push({now + T[g].plane_delay, 0, g});
+      if (pcount[g + 1] > pcount[g]) ev.push({now + T[g].plane_delay, 0, g});  // else it releases nothing
       while (cur < ncls && cls_left[cur] == 0) ++cur;
     }
     if (ev.empty()) break;
