@@ -377,6 +377,15 @@ class Problem:
                                           ctypes.byref(self.quan), ctypes.byref(self.env)))
         return vo
 
+    def sweep_host_ptr(self, vo_ptr: int, vi_ptr: int) -> None:
+        """Sweeper_sweep on host buffers given by address (e.g. pinned torch
+        tensors): the reference driver's call, host vi in, host vo out."""
+        n = self.nstate
+        pvi = Pointer(n, vi_ptr, None, 0, 1, 0)
+        pvo = Pointer(n, vo_ptr, None, 0, 1, 0)
+        _check(lib().Sweeper_sweep_status(ctypes.byref(self.sweeper), ctypes.byref(pvo), ctypes.byref(pvi),
+                                          ctypes.byref(self.quan), ctypes.byref(self.env)))
+
     def sweep_device(self, vo_ptr: int, vi_ptr: int) -> None:
         """Enqueue vo = sweep(vi) on device arrays (async on self.stream)."""
         _check(lib().Sweeper_sweep_device(ctypes.byref(self.sweeper), ctypes.c_void_p(vo_ptr),
