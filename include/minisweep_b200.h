@@ -336,8 +336,8 @@ int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const double* v_
                              const Quantities* quan, Env* env);
 /* Group-pair slices the last host-buffer call (Sweeper_sweep[_status] or
  * Sweeper_sweep_iterations) ran in (1: the whole problem at once; 0: no call
- * yet).  On a large FP64 problem (state of 256 MiB or more, 16 or more group
- * pairs) those calls sweep the groups in up to 4 slices, each through every
+ * yet).  On a large problem (FP64 or mixed precision; state of 256 MiB or
+ * more, 16 or more group pairs) those calls sweep the groups in up to 4 slices, each through every
  * iteration, so that a slice's host copies overlap the other slices' sweeps;
  * the results are the same.  No reference counterpart. */
 int msb_iterations_slices(const Sweeper* sweeper);

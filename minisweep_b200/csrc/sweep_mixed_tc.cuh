@@ -945,28 +945,31 @@ __global__ void __launch_bounds__(MixCfg<NM_, NS>::NT, 1) sweep_mixed_kernel(con
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TM_COLS) : "memory");
 }
 
-// vi -> vi16, once per sweep: thread t converts moment chunk `half` (moments
-// 8 half .. 8 half + 7, zero padded) of row r8 = 4 g + u of block t / 16
-// (cell (ix, iy, iz), group pair gp; group 2 gp + g, unknown u).  The chunk
+// vi -> vi16, once per sweep, for the group pairs [gp0, gp1): thread t
+// converts moment chunk `half` (moments 8 half .. 8 half + 7, zero padded) of
+// row r8 = 4 g + u of the (t / 16)-th block of that range (cell (ix, iy, iz),
+// group pair gp; group 2 gp + g, unknown u).  The chunk
 // is scaled by 2^k1 so that its largest entry lies in [2^14, 2^15) (k1
 // clamped to [-120, 120]), rounded to FP32 in FP64 and split into hi + lo
 // 16-bit halves -- the operand every octant's first transform of that cell
 // uses.  A group beyond ne (odd ne) and the chunks beyond NM are zeros.
 template <int NM_, int FMT>
 __global__ void __launch_bounds__(256) convert_vi16(const double* __restrict__ vi, unsigned char* __restrict__ out,
-                                                    int nx, int ny, int nz, int ne, int ngp) {
+                                                    int nx, int ny, int nz, int ne, int ngp, int gp0, int gp1) {
   using H = Half16<FMT>;
   constexpr int NMC = NM_ < 8 ? NM_ : 8;  // moments of a chunk
-  const long long nunit = (long long)nx * ny * nz * ngp * 16;
+  const int ngr = gp1 - gp0;  // the group pairs converted: [gp0, gp1)
+  const long long nunit = (long long)nx * ny * nz * ngr * 16;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nunit;
        t += (long long)gridDim.x * blockDim.x) {
     const int r8 = (int)(t & 7), half = (int)((t >> 3) & 1);
-    const long long blk = t >> 4;
-    const int ix = (int)(blk % nx);
-    long long q = blk / nx;
+    long long q = t >> 4;
+    const int ix = (int)(q % nx);
+    q /= nx;
     const int iy = (int)(q % ny);
     q /= ny;
-    const int gp = (int)(q % ngp), iz = (int)(q / ngp);
+    const int gp = gp0 + (int)(q % ngr), iz = (int)(q / ngr);
+    const long long blk = (((long long)iz * ngp + gp) * ny + iy) * nx + ix;
     const int g = r8 >> 2, u = r8 & 3, ie = 2 * gp + g;
     int k1 = 0;
     uint32_t hi[4] = {0u, 0u, 0u, 0u}, lo[4] = {0u, 0u, 0u, 0u};
@@ -1001,16 +1004,24 @@ __global__ void __launch_bounds__(256) convert_vi16(const double* __restrict__ v
 
 // vo = sum over the eight octants of their FP32 partials, in FP64 and in
 // octant order (deterministic); with `accumulate` the sum is added to vo (the
-// angle passes after the first of a larger na).  n is a multiple of 4
-// (NM * NU elements per (cell, group)).
+// angle passes after the first of a larger na).  The elements summed are
+// iz * zstride + off + [0, width) for iz in [0, nz): one contiguous run of
+// groups per z-plane (the whole state: zstride = width, off = 0).  width,
+// zstride and off are multiples of 4 (NM * NU elements per (cell, group)).
 __global__ void __launch_bounds__(256) reduce_octant_partials(double* __restrict__ vo,
-                                                              const float* __restrict__ part, size_t n,
-                                                              int accumulate) {
-  const size_t n4 = n / 4;
+                                                              const float* __restrict__ part, size_t state,
+                                                              int accumulate, size_t zstride, size_t off,
+                                                              size_t width, int nz) {
+  const size_t w4 = width / 4, n4 = w4 * (size_t)nz;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    size_t e4 = off / 4 + i;  // in units of 4 elements; one run when the groups are all of them
+    if (zstride != width) {
+      const size_t iz = i / w4;
+      e4 = (iz * zstride + off) / 4 + (i - iz * w4);
+    }
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if (accumulate) {
-      const double2* d = reinterpret_cast<const double2*>(vo) + 2 * i;
+      const double2* d = reinterpret_cast<const double2*>(vo) + 2 * e4;
       const double2 p0 = __ldcs(d), p1 = __ldcs(d + 1);
       a0 = p0.x;
       a1 = p0.y;
@@ -1019,13 +1030,13 @@ __global__ void __launch_bounds__(256) reduce_octant_partials(double* __restrict
     }
 #pragma unroll
     for (int o = 0; o < NOCTANT; ++o) {
-      const float4 q = __ldcs(reinterpret_cast<const float4*>(part + n * o) + i);
+      const float4 q = __ldcs(reinterpret_cast<const float4*>(part + state * o) + e4);
       a0 = __dadd_rn(a0, (double)q.x);
       a1 = __dadd_rn(a1, (double)q.y);
       a2 = __dadd_rn(a2, (double)q.z);
       a3 = __dadd_rn(a3, (double)q.w);
     }
-    double2* d = reinterpret_cast<double2*>(vo) + 2 * i;
+    double2* d = reinterpret_cast<double2*>(vo) + 2 * e4;
     __stcs(d, make_double2(a0, a1));
     __stcs(d + 1, make_double2(a2, a3));
   }

@@ -27,7 +27,7 @@ namespace {
 
 using KernelFn = void (*)(const Fp64Params);
 using MixKernelFn = void (*)(const MixParams);
-using MixConvFn = void (*)(const double*, unsigned char*, int, int, int, int, int);
+using MixConvFn = void (*)(const double*, unsigned char*, int, int, int, int, int, int, int);
 
 // One compiled kernel: the FP64 kernel (fn) or a mixed-precision one (mix).
 struct Variant {
@@ -470,16 +470,20 @@ static int launch_fp64(SweeperImpl& S, const Variant& var, const int* d_tasks, l
 
 // Every pass of one mixed-precision sweep: per pass the sweep kernel writes
 // each octant's FP32 contribution, and the partial sum adds them up in vo.
-static int launch_mixed(SweeperImpl& S, double* vo_d, const double* vi_d, cudaStream_t stream) {
+// The tasks given may be those of the group pairs [gp0, gp1) only (a slice of
+// a host-buffer run); the conversion and the sum then cover those groups.
+static int launch_mixed(SweeperImpl& S, double* vo_d, const double* vi_d, cudaStream_t stream,
+                        const int* d_tasks, long long ntask, int gp0, int gp1) {
   const int na = S.dims.na, pa = pass_angles(S), npass = (na + pa - 1) / pa;
+  const Dimensions& d = S.dims;
   MixParams P;
-  fill_params<float>(S, P, P, vi_d, S.d_tasks, S.sched.ntask());
+  fill_params<float>(S, P, P, vi_d, d_tasks, ntask);
   P.part = S.d_part;
   P.state = S.part_elems / NOCTANT;
   int rc;
   // vi in the first transform's operand format, once for every octant and pass
-  S.var.conv<<<S.nsm * 8, 256, 0, stream>>>(vi_d, S.d_vi16, S.dims.ncell_x, S.dims.ncell_y, S.dims.ncell_z,
-                                            S.dims.ne, S.ngp);
+  S.var.conv<<<S.nsm * 8, 256, 0, stream>>>(vi_d, S.d_vi16, d.ncell_x, d.ncell_y, d.ncell_z, d.ne, S.ngp, gp0,
+                                            gp1);
   if ((rc = cuda_check(cudaGetLastError(), "vi conversion launch"))) return rc;
   P.vi16 = S.d_vi16;
   for (int c = 0; c < npass; ++c) {
@@ -494,7 +498,10 @@ static int launch_mixed(SweeperImpl& S, double* vo_d, const double* vi_d, cudaSt
     }
     S.var.mix<<<S.grid, S.var.threads, S.var.smem, stream>>>(P);
     if ((rc = cuda_check(cudaGetLastError(), "sweep kernel launch"))) return rc;
-    reduce_octant_partials<<<S.nsm * 8, 256, 0, stream>>>(vo_d, S.d_part, P.state, c > 0 ? 1 : 0);
+    const size_t layer = (size_t)d.nm * NU * d.ncell_x * d.ncell_y;  // one (iz, ie) slab
+    const int e0 = 2 * gp0, e1 = std::min(2 * gp1, d.ne);
+    reduce_octant_partials<<<S.nsm * 8, 256, 0, stream>>>(vo_d, S.d_part, P.state, c > 0 ? 1 : 0, layer * d.ne,
+                                                          layer * e0, layer * (e1 - e0), d.ncell_z);
     if ((rc = cuda_check(cudaGetLastError(), "partial sum launch"))) return rc;
   }
   return MSB_OK;
@@ -598,7 +605,7 @@ static int impl_sweep(SweeperImpl& S, double* vo_d, const double* vi_d, const do
   } else if (S.var.fn) {
     if ((rc = launch_fp64(S, S.var, S.d_tasks, S.sched.ntask(), S.grid, vo_d, vi_d, stream))) return rc;
   } else {
-    if ((rc = launch_mixed(S, vo_d, vi_d, stream))) return rc;
+    if ((rc = launch_mixed(S, vo_d, vi_d, stream, S.d_tasks, S.sched.ntask(), 0, S.ngp))) return rc;
   }
   if ((rc = cuda_check(cudaMemcpyAsync(S.h_status, S.d_sync, 4 * sizeof(int), cudaMemcpyDeviceToHost, stream),
                        "status copy")))
@@ -621,15 +628,16 @@ static int impl_sync(SweeperImpl& S, cudaStream_t stream) {
 
 // ------------------------------------------- host-buffer runs in group slices
 // The energy groups are independent in the sweep (no face, dependency or sum
-// crosses them), so a run of Sweeper_sweep_iterations on a large FP64 problem
-// is split into slices of group pairs, each swept through every iteration
+// crosses them), so a run of Sweeper_sweep_iterations on a large problem
+// (FP64, or mixed precision: the vi conversion and the partial sum then cover
+// the slice's groups) is split into slices of group pairs, each swept through every iteration
 // with its own task table: the host->device copy of slice k + 1 then runs
 // while slice k is swept, and the device->host copy of slice k while slice
 // k + 1 is.  Every value is the one the unsliced run computes.  Slices are
 // used only where they stay efficient (64^3 cells x na 32, one B200: 115.9 ms
 // per sweep with 64 groups, 58.2 with 32, 29.8 with 16, 16.4 with 8).
 static int slice_count(const SweeperImpl& S) {
-  if (S.kba || !S.var.fn || (S.autotune && !S.tuned)) return 1;
+  if (S.kba || !S.var.valid() || (S.autotune && !S.tuned)) return 1;
   const size_t bytes = Dimensions_size_state(S.dims, NU) * sizeof(double);
   if (bytes < ((size_t)256 << 20)) return 1;  // copies too short to be worth hiding
   return std::max(1, std::min(4, S.ngp / 8));
@@ -749,7 +757,9 @@ static int sweep_iterations_sliced(SweeperImpl& S, int nslice, double* out_h, co
     double* b = d_b;
     for (int it = 0; it < niterations && !rc; ++it) {
       if (k > 0 || it > 0) rc = reset_pass(S, st);
-      if (!rc) rc = launch_fp64(S, S.var, T.d_tasks[k], T.ntask[k], S.grid, b, a, st);
+      if (!rc)
+        rc = S.var.fn ? launch_fp64(S, S.var, T.d_tasks[k], T.ntask[k], S.grid, b, a, st)
+                      : launch_mixed(S, b, a, st, T.d_tasks[k], T.ntask[k], T.gp0[k], T.gp0[k + 1]);
       std::swap(a, b);
     }
     if (!rc) rc = cuda_check(cudaEventRecord(ev[1 + nslice + k], st), "slice event");
@@ -776,7 +786,7 @@ static int sweep_iterations_sliced(SweeperImpl& S, int nslice, double* out_h, co
   if (sd) cudaStreamDestroy(sd);
   if (!rc) {
     const int npass = (d.na + pass_angles(S) - 1) / pass_angles(S);
-    S.nlaunch = npass;
+    S.nlaunch = S.var.mix ? 1 + 2 * npass : npass;  // of the last sweep
   }
   return rc;
 }
@@ -1315,7 +1325,7 @@ extern "C" int Sweeper_set_spin_limit(Sweeper* sweeper, long long limit) {
 // the device: v_in_h (host) is copied in once, niterations sweeps ping-pong
 // between two device arrays (the vi/vo swap), and the last sweep's output is
 // copied to v_out_h.  Pinned host buffers make the copies asynchronous; on a
-// large FP64 problem the run goes in group-pair slices whose copies overlap
+// large problem the run goes in group-pair slices whose copies overlap
 // the other slices' sweeps (sweep_iterations_sliced).
 extern "C" int Sweeper_sweep_iterations(Sweeper* sweeper, double* v_out_h, const double* v_in_h, int niterations,
                                         const Quantities* quan, Env* env) {

@@ -66,6 +66,26 @@ def test_iterations_match_device_sweeps(nx, ny, nz, ne, na, nm, niter, slices):
     assert np.array_equal(got, ref), f"max abs diff {np.max(np.abs(got - ref))}"
 
 
+@pytest.mark.parametrize("nx,ny,nz,ne,na,prec,niter", [
+    (32, 32, 32, 32, 32, 1, 2),   # FP16 halves, 2 slices
+    (32, 32, 32, 33, 64, 2, 1),   # BF16 halves, odd ne, two angle passes (the partial sum adds)
+])
+def test_mixed_iterations_sliced(nx, ny, nz, ne, na, prec, niter):
+    """The mixed-precision sweeper goes in slices too: the vi conversion and
+    the partial sum cover each slice's groups, and the results are those of
+    the whole-problem sweeps, bit for bit."""
+    with msb.Problem(flags(nx, ny, nz, ne, na, f"--precision {prec}"), nm=16) as pb:
+        vi = random_state(pb, 8)
+        ref = device_iterations(pb, vi, niter)
+        got = host_iterations(pb, vi, niter)
+        assert pb.iterations_slices() == 2
+        one = pb.sweep_host(vi)
+        assert pb.iterations_slices() == 2
+        ref1 = device_iterations(pb, vi, 1)
+    assert np.array_equal(got, ref), f"max abs diff {np.max(np.abs(got - ref))}"
+    assert np.array_equal(one, ref1)
+
+
 def test_host_pointer_sweep_sliced():
     """Sweeper_sweep (host Pointers, the reference driver's call) goes in
     slices too."""
